@@ -1,0 +1,131 @@
+/*
+ * simba_b200 -- C ABI of the B200-native SIMBA / VFB search library
+ * (libsimba_b200.so).  Plain C types only; every buffer is owned by the
+ * caller; no call throws or aborts across this boundary.
+ *
+ * The reference exposes no library API: its only interface is the two
+ * executables `simba <instance.json> <maxLen>` (simba/src/nocache.cu:291-342)
+ * and `vfb <instance.json> <maxLen>` (vfb/src/full-cache.cu:776-854).  Each
+ * entry point below names the reference code it replaces.
+ */
+#ifndef SIMBA_B200_H
+#define SIMBA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SIMBA_ABI_VERSION 1
+
+/* Status codes (return value of the solve calls and result.status). */
+#define SIMBA_OK 0           /* an expression was found                      */
+#define SIMBA_NOT_FOUND 1    /* every size searched, no match: "Not found !" */
+#define SIMBA_BUDGET 2       /* time budget exhausted before a match         */
+#define SIMBA_CACHE_FULL 3   /* VFB cache capacity reached: "Not found !"    */
+#define SIMBA_E_ARG (-1)     /* bad argument or limit exceeded               */
+#define SIMBA_E_CUDA (-2)    /* CUDA runtime error                           */
+#define SIMBA_E_NOMEM (-3)   /* device or host allocation failed             */
+#define SIMBA_E_NODEV (-4)   /* no usable CUDA device                        */
+#define SIMBA_E_OVERFLOW (-5)/* a candidate count exceeds 64 bits            */
+#define SIMBA_E_INTERNAL (-6)/* internal consistency check failed            */
+#define SIMBA_E_IO (-7)      /* instance file unreadable or malformed        */
+
+/* One MBA learning instance.  Mirrors MbaInstance (simba/src/instance.h:10-30):
+ * inputs are sample-major, inputs[i * num_variables + j] = variable j on
+ * sample i.  A constant terminal 1 is an extra variable equal to 1 on every
+ * sample.  word_bits selects the arithmetic: 32 (the reference's uint32_t,
+ * simba/src/mba.cuh:8) or 64 (exact uint64, mod 2^64). */
+typedef struct {
+  int32_t num_variables;
+  int32_t num_examples;
+  int32_t word_bits;
+  int32_t reserved;
+  const uint64_t *inputs;
+  const uint64_t *outputs;
+} simba_instance;
+
+/* Options; a zero-filled struct (or NULL) gives the reference behaviour. */
+typedef struct {
+  int32_t device;        /* CUDA device ordinal                                  */
+  int32_t size_range;    /* 0: sizes 2..max-1 like the reference (nocache.cu:246);
+                            1: sizes 1..max                                       */
+  int32_t verbose;       /* progress lines on stderr                             */
+  int32_t engine;        /* 0: tabled spine engine; 1: one thread per rank       */
+  double budget_seconds; /* 0 = unlimited                                        */
+  int64_t table_bytes;   /* cap on the value tables, 0 = default (4 GiB)         */
+  uint64_t stream;       /* cudaStream_t to launch on (0 = library-owned stream)  */
+  int32_t reserved[6];
+} simba_options;
+
+typedef struct {
+  int32_t status;
+  int32_t size;          /* size of the expression found                         */
+  int32_t op;            /* root-operator block 0..7 (~ & | ^ neg + - *), 8 = leaf */
+  int32_t table_size;    /* largest tabled size used by the engine               */
+  uint64_t rank;         /* minimum matching rank of that size                   */
+  char postfix[64];      /* reference encoding: '0'+var and ~ & | ^ # + - *      */
+  char expr[512];        /* SIMBA syntax, e.g. (v0 + (~v1))  (nocache.cu:162-195) */
+  double seconds;        /* wall time of the call                                */
+  double device_ms;      /* GPU time of the search kernels                       */
+  uint64_t candidates;   /* candidates in the blocks searched (reference rule)   */
+  uint64_t evaluated;    /* candidates the kernels evaluated                     */
+  uint64_t per_size[33]; /* candidates per size (reference rule)                 */
+  int32_t max_size_searched;
+  int32_t launches;      /* kernels launched by the call                         */
+  double kernel_ms;      /* GPU time of the search kernel launches alone         */
+  uint64_t alg_ops;      /* integer lane-operations the algorithm needs for the
+                            candidates evaluated (see simba_int_peak)            */
+} simba_result;
+
+/* Plain cache-free unranking search of one instance: replaces NoCache::solve
+ * (simba/src/nocache.cu:197-289).  Searches sizes in increasing order and
+ * operator blocks in the reference order, stops after the first block that
+ * holds a match and returns the minimum matching rank of that block.
+ * Returns result.status. */
+int simba_solve(const simba_instance *inst, int max_size, const simba_options *opt,
+                simba_result *result);
+
+/* Resident session: samples and value tables stay on the device between
+ * calls (used by the benchmark to time the search with inputs in HBM). */
+typedef struct simba_session simba_session;
+int simba_session_create(const simba_instance *inst, const simba_options *opt,
+                         simba_session **session);
+int simba_session_solve(simba_session *session, int max_size, simba_result *result);
+/* Evaluate every candidate of sizes lo..hi with no early stop (throughput). */
+int simba_session_sweep(simba_session *session, int lo, int hi, simba_result *result);
+void simba_session_destroy(simba_session *session);
+
+/* Count table numForm[size][op] (simba/src/nocache.cu:117-160), written as
+ * (max_size + 1) rows of 9 columns, column 8 = total.  Host only. */
+int simba_count_table(int max_size, int n_terms, uint64_t *table);
+/* Rank -> postfix (simba/src/nocache.cu:23-83); writes size chars + NUL. */
+int simba_unrank(uint64_t rank, int size, int n_terms, char *postfix);
+/* Postfix -> rank (inverse of simba_unrank). */
+int simba_rank_of(const char *postfix, int n_terms, uint64_t *rank);
+/* Postfix -> infix; style 0 = SIMBA (nocache.cu:162-195), 1 = VFB
+ * (vfb/src/full-cache.cu:483-509).  Returns the length or a negative code. */
+int simba_format(const char *postfix, int style, char *out, int cap);
+
+/* Instance file reader: the reference JSON schema (simba/src/instance.cpp:7-27,
+ * vfb/src/utils.h:15-44); "size": 64 on the values selects 64-bit words.
+ * The arrays are owned by the library until simba_instance_free. */
+int simba_instance_load(const char *path, simba_instance *inst);
+void simba_instance_free(simba_instance *inst);
+
+/* Measured integer-ALU issue rate of the device: independent 32-bit
+ * LOP3/IADD3 chains over every SM, in lane-operations per second.  The
+ * denominator of the search kernels' roofline (no counterpart in the
+ * reference, which reports no roofline). */
+int simba_int_peak(int device, double *lane_ops_per_s);
+
+const char *simba_version(void);
+const char *simba_status_string(int status);
+const char *simba_last_error(void);
+int simba_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SIMBA_B200_H */

@@ -1,0 +1,83 @@
+// Internal C++ interface between the C ABI (capi.cpp) and the CUDA engines
+// (search.cu, vfb.cu, batch.cu).  Nothing here crosses the library boundary.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/simba_b200.h"
+#include "grammar.h"
+
+namespace simba {
+
+// An instance with its words already reduced to the word width.
+struct HostInstance {
+  int k = 0;          // terminals
+  int S = 0;          // samples
+  int bits = 32;      // 32 or 64
+  std::vector<uint64_t> in;   // S*k sample-major
+  std::vector<uint64_t> out;  // S
+};
+
+struct EngineOptions {
+  int device = 0;
+  int size_range = 0;        // 0 reference (2..max-1), 1 complete (1..max)
+  int verbose = 0;
+  double budget_s = 0.0;     // 0 = unlimited
+  int64_t table_bytes = 0;   // 0 = default cap
+  int engine = 0;            // 0 spine (auto), 1 naive per-rank kernel
+  int stop_on_match = 1;     // 0: evaluate whole sizes (throughput sweeps)
+  uint64_t stream = 0;       // caller's cudaStream_t, 0 = own stream
+};
+
+// Per-solve outcome filled by the engines (capi.cpp formats the strings).
+struct SolveOutcome {
+  int status = SIMBA_NOT_FOUND;
+  int size = 0;
+  int op = -1;
+  uint64_t rank = 0;
+  std::string postfix;
+  double device_ms = 0.0;
+  uint64_t candidates = 0;
+  uint64_t evaluated = 0;
+  uint64_t per_size[kMaxSize + 1] = {};
+  int table_size = 0;
+  int max_size_searched = 0;
+  int launches = 0;
+  double kernel_ms = 0.0;
+  uint64_t alg_ops = 0;
+};
+
+std::string last_error();
+void set_last_error(const std::string& e);
+
+// Limits check shared by every entry point (the reference's own limits are
+// 10 variables / 100 samples / size 32: simba/src/globals.cuh:5-7; this
+// build allows kMaxTerms / kMaxSamples / kMaxSize).
+int validate(const HostInstance& h, int max_size);
+
+// Plain SIMBA search on one instance.  Session objects keep the samples and
+// value tables resident between calls.
+class SearchSession {
+ public:
+  virtual ~SearchSession() = default;
+  virtual int solve(int max_size, SolveOutcome* out) = 0;
+  // Evaluate every candidate of sizes [lo, hi] with no early stop.
+  virtual int sweep(int lo, int hi, SolveOutcome* out) = 0;
+};
+
+int make_search_session(const HostInstance& h, const EngineOptions& o,
+                        SearchSession** out);
+
+// Read an instance file in the reference JSON schema.
+int read_instance_json(const std::string& path, HostInstance* h);
+
+int measure_int_peak(int device, double* lane_ops_per_s);
+
+// Format a postfix string in the SIMBA (style 0) or VFB (style 1) syntax.
+std::string format_postfix(const std::string& postfix, int style);
+
+// Host-side exact check of an expression on every sample.
+bool host_check(const std::string& postfix, const HostInstance& h);
+
+}  // namespace simba

@@ -1,0 +1,1149 @@
+// Plain SIMBA search on sm_100a: tabled spine engine + one-thread-per-rank
+// engine.
+//
+// What is computed is exactly the reference's search (simba/src/nocache.cu:
+// 197-289): sizes in increasing order, the rank space of each size in the
+// reference order, stop after the first (size, root-operator) block holding
+// an expression that matches every sample, and report the minimum matching
+// rank of that block.
+//
+// How it is computed differs.  The reference unranks every rank from
+// scratch and interprets the postfix string (nocache.cu:23-107,
+// mba.cuh:6-69).  Here:
+//
+//  * Value tables.  V_t[r] = value on sample 0 of the size-t expression of
+//    rank r, for every t <= T, built bottom-up (one operator per entry) in
+//    HBM.  Building V_t is itself the search of size t.
+//  * Spines.  A candidate of size s > T is a path from the root along its
+//    larger operand ("big side") down to a subtree of size <= T (the
+//    "bottom", read from V_tb); every level on the path combines the big
+//    side with a "small side" of size <= T (read from V_ts), or applies a
+//    chain of unary operators.  A spine shape with fixed small-side indices
+//    is a "context"; its candidates are all bottom values v in V_tb, and
+//    their ranks are base + sum(idx_l * coef_l) + v * coefv, so the whole
+//    rank space of a size is a disjoint union of (context x bottom range)
+//    rectangles.  Unary chains that compose to the same affine map
+//    (x -> +-x + c) are tested once with the smallest of their ranks, which
+//    yields the same minimum matching rank.
+//  * Inversion.  The sample-0 test "root value == target" is pushed down
+//    the spine into a constraint "(v & M) == K" on the bottom value, so a
+//    candidate costs one load (amortised over R contexts) and one masked
+//    compare.  Operators that cannot be inverted under the mask left by
+//    & / | above them are evaluated explicitly instead.
+//  * Verification.  A sample-0 match is queued in shared memory and then
+//    verified by a whole warp: each lane evaluates different samples (staged
+//    in shared memory) and a ballot rejects the candidate at the first
+//    mismatching group of samples.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "cuda_util.h"
+#include "engine.h"
+#include "grammar.h"
+
+namespace simba {
+
+constexpr int kMaxDepth = 12;  // spine levels
+constexpr int kThreads = 256;  // CTA size of the search kernels
+constexpr int kQueue = 128;    // shared-memory queue of sample-0 matches
+constexpr int kR = 4;          // contexts per thread
+constexpr int kMaxExplicit = 4;
+
+// One level of a spine, top-down (level 0 is the root).
+struct Level {
+  uint64_t coef;     // rank coefficient of this level's small index
+  uint64_t nsmall;   // N(ts) (binary), 1 (chain)
+  uint64_t c;        // chain: additive constant (two's complement)
+  int8_t kind;       // 0 binary, 1 unary chain x -> eps * x + c
+  int8_t op;         // binary operator
+  int8_t small_left; // small operand is the left one
+  int8_t ts;         // small side size
+  int8_t eps;        // chain sign
+  int8_t pad[3];
+};
+
+struct Item {
+  uint64_t base;        // rank of the all-zero indices
+  uint64_t coefv;       // rank coefficient of the bottom index
+  uint64_t nctx;        // number of contexts
+  uint64_t nv;          // bottom values N(tb)
+  uint64_t unit_begin;  // first work unit of this item
+  uint64_t vb;          // bottom values per unit (multiple of 64)
+  uint64_t cblocks;     // context blocks
+  uint64_t vblocks;     // value blocks
+  uint32_t cb;          // contexts per unit = G * kR
+  uint16_t G, L;        // G context groups x L value lanes = kThreads
+  int8_t depth, inv, bottom, full, nexp;
+  int8_t pad[19];
+  Level lv[kMaxDepth];
+};
+static_assert(sizeof(Item) % 16 == 0, "Item must be 16-byte sized");
+
+template <class W>
+struct Params {
+  const W* tab[kMaxSize + 1];
+  const Item* items;
+  const W* in;
+  const W* out;
+  const unsigned long long* counts;
+  unsigned long long* counter;
+  unsigned long long* best;
+  unsigned long long* evaluated;
+  unsigned long long* start_ns;
+  int* flags;  // [0] budget expired, [1] inversion failure, [2] queue overflows
+  unsigned long long total_units;
+  unsigned long long budget_ns;
+  W target;
+  int nitems;
+  int size;
+  int S, K;
+  int stop_on_match;
+};
+
+struct Smem {
+  unsigned long long counts[(kMaxSize + 1) * kCols];
+  Item item;
+  unsigned long long queue[kQueue];
+  unsigned long long unit;
+  int qn;
+  int item_idx;
+  int next_item;
+  int skip;
+  char post[kThreads / 32][kMaxSize + 8];
+};
+
+// ------------------------------------------------------------------ device ops
+
+__host__ __device__ __forceinline__ unsigned long long umin64(unsigned long long a,
+                                                             unsigned long long b) {
+  return a < b ? a : b;
+}
+
+template <class W>
+__device__ __forceinline__ W bin_apply(int op, W l, W r) {
+  switch (op) {
+    case OP_AND: return l & r;
+    case OP_OR: return l | r;
+    case OP_XOR: return l ^ r;
+    case OP_ADD: return l + r;
+    case OP_SUB: return l - r;
+    default: return l * r;  // OP_MUL
+  }
+}
+
+template <class W>
+__device__ __forceinline__ W un_apply(int op, W x) {
+  return op == OP_NOT ? (W)~x : (W)(W(0) - x);
+}
+
+// Multiplicative inverse of an odd word modulo 2^bits by Newton iteration
+// x <- x (2 - a x), which doubles the number of correct low bits each step.
+template <class W>
+__host__ __device__ __forceinline__ W odd_inverse(W a) {
+  W x = a;  // correct to 3 bits for odd a
+#pragma unroll
+  for (int i = 0; i < 5; ++i) x *= (W)2 - a * x;
+  return x;
+}
+
+template <class W>
+__device__ __forceinline__ int word_ctz(W w) {
+  if (sizeof(W) == 8) return w ? __ffsll((long long)w) - 1 : 64;
+  return w ? __ffs((int)w) - 1 : 32;
+}
+
+template <class W>
+__device__ __forceinline__ int word_popc(W w) {
+  return sizeof(W) == 8 ? __popcll((unsigned long long)w) : __popc((unsigned)w);
+}
+
+// Push the constraint (y & M) == K through one level y = f(w, x) to a
+// constraint on x.  Infeasible constraints become M = 0, K = 1.  Returns
+// false if the level is arithmetic and M is not of the form 2^n - 1.
+template <class W>
+__device__ bool invert_level(const Level& L, W w, W& M, W& K) {
+  if (M == 0 && K != 0) return true;
+  const bool low = (M & (M + 1)) == 0;
+  if (L.kind == 1) {
+    const W c = (W)L.c;
+    if (L.eps < 0 && c == (W)~W(0)) {  // ~x
+      K = (W)~K & M;
+      return true;
+    }
+    if (!low) return false;
+    K = (L.eps > 0 ? (W)(K - c) : (W)(c - K)) & M;
+    return true;
+  }
+  switch (L.op) {
+    case OP_XOR:
+      K = (K ^ w) & M;
+      return true;
+    case OP_AND:
+      if (K & (W)~w) { M = 0; K = 1; }
+      else M &= w;
+      return true;
+    case OP_OR:
+      if (w & M & (W)~K) { M = 0; K = 1; }
+      else { M &= (W)~w; K &= (W)~w; }
+      return true;
+    case OP_ADD:
+      if (!low) return false;
+      K = (W)(K - w) & M;
+      return true;
+    case OP_SUB:
+      if (!low) return false;
+      K = (L.small_left ? (W)(w - K) : (W)(K + w)) & M;
+      return true;
+    case OP_MUL: {
+      if (!low) return false;
+      const int n = word_popc<W>(M);
+      const int e = word_ctz<W>(w);
+      if (e >= n) {
+        if (K != 0) { M = 0; K = 1; }
+        else { M = 0; K = 0; }
+        return true;
+      }
+      if (e > 0 && (K & (((W)1 << e) - 1))) { M = 0; K = 1; return true; }
+      const W inv = odd_inverse<W>((W)(w >> e));
+      M = (W)(M >> e);
+      K = (W)((W)(K >> e) * inv) & M;
+      return true;
+    }
+  }
+  return false;
+}
+
+template <class W>
+__device__ __forceinline__ W level_apply(int kind, int op, int small_left, int eps, W c, W w,
+                                         W y) {
+  if (kind == 1) return eps > 0 ? (W)(y + c) : (W)(c - y);
+  return small_left ? bin_apply<W>(op, w, y) : bin_apply<W>(op, y, w);
+}
+
+// Evaluate a postfix expression on one sample row (k words in shared memory).
+template <class W>
+__device__ W eval_postfix(const char* p, int len, const W* row) {
+  W st[kMaxSize + 1];
+  int sp = -1;
+  for (int j = 0; j < len; ++j) {
+    const char ch = p[j];
+    const int op = char_op(ch);
+    if (op < 0) {
+      st[++sp] = row[ch - '0'];
+    } else if (is_unary(op)) {
+      st[sp] = un_apply<W>(op, st[sp]);
+    } else {
+      const W r = st[sp--];
+      st[sp] = bin_apply<W>(op, st[sp], r);
+    }
+  }
+  return st[0];
+}
+
+// Single-thread verification on every sample (used when the queue is full).
+template <class W>
+__device__ bool thread_verify(const Params<W>& p, const Smem& sm, const W* s_in, const W* s_out,
+                              unsigned long long rank) {
+  char post[kMaxSize + 1];
+  unrank(rank, p.size, (const uint64_t(*)[kCols])sm.counts, post);
+  for (int i = 0; i < p.S; ++i)
+    if (eval_postfix<W>(post, p.size, s_in + i * p.K) != s_out[i]) return false;
+  return true;
+}
+
+// Warp-cooperative verification of the queued sample-0 matches: lane i
+// checks samples i, i+32, ...; a ballot after each group of 32 samples
+// rejects the candidate at the first mismatch.
+template <class W>
+__device__ void verify_queue(const Params<W>& p, Smem& sm, const W* s_in, const W* s_out) {
+  const int nq = min(sm.qn, kQueue);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int h = warp; h < nq; h += kThreads / 32) {
+    const unsigned long long rank = sm.queue[h];
+    unsigned long long cur = 0;
+    if (lane == 0) cur = *(volatile unsigned long long*)p.best;
+    cur = __shfl_sync(0xffffffffu, cur, 0);
+    if (rank >= cur) continue;
+    char* post = sm.post[warp];
+    if (lane == 0) unrank(rank, p.size, (const uint64_t(*)[kCols])sm.counts, post);
+    __syncwarp();
+    bool all_ok = true;
+    for (int base = 0; base < p.S; base += 32) {
+      const int i = base + lane;
+      bool ok = true;
+      if (i < p.S) ok = eval_postfix<W>(post, p.size, s_in + i * p.K) == s_out[i];
+      if (__ballot_sync(0xffffffffu, !ok)) { all_ok = false; break; }
+    }
+    if (all_ok && lane == 0) atomicMin(p.best, rank);
+    __syncwarp();
+  }
+}
+
+// Decode context index c into small-side indices (deepest level fastest)
+// and return its rank base; optionally fetch the small values.
+template <class W>
+__device__ __forceinline__ unsigned long long decode_context(const Params<W>& p, const Item& it,
+                                                             unsigned long long c, W* wl) {
+  unsigned long long rank = it.base;
+  for (int l = it.depth - 1; l >= 0; --l) {
+    const Level& L = it.lv[l];
+    if (L.kind != 0) continue;
+    const unsigned long long idx = c % L.nsmall;
+    c /= L.nsmall;
+    rank += idx * L.coef;
+    if (wl) wl[l] = p.tab[L.ts][idx];
+  }
+  return rank;
+}
+
+template <class W>
+__device__ __forceinline__ void push_hit(const Params<W>& p, Smem& sm, const W* s_in,
+                                         const W* s_out, unsigned long long rank) {
+  const int i = atomicAdd(&sm.qn, 1);
+  if (i < kQueue) {
+    sm.queue[i] = rank;
+  } else {
+    atomicAdd(&p.flags[2], 1);
+    if (thread_verify<W>(p, sm, s_in, s_out, rank)) atomicMin(p.best, rank);
+  }
+}
+
+template <class W>
+struct Explicit {
+  int kind[kMaxExplicit], op[kMaxExplicit], sl[kMaxExplicit], eps[kMaxExplicit];
+  W c[kMaxExplicit];
+};
+
+// Bottom-up evaluation of the levels the inversion could not absorb.
+template <class W, int E>
+__device__ __forceinline__ W eval_explicit(const Explicit<W>& X, const W* w, W x) {
+  W y = x;
+#pragma unroll
+  for (int j = E - 1; j >= 0; --j) y = level_apply<W>(X.kind[j], X.op[j], X.sl[j], X.eps[j], X.c[j], w[j], y);
+  return y;
+}
+
+// One work unit: kR contexts per thread x a strided share of the bottom
+// values.  Loads are 16-byte vectors of the bottom table.
+template <class W, int E, bool FULL>
+__device__ void process_unit(const Params<W>& p, Smem& sm, const Item& it, unsigned long long local,
+                             const W* s_in, const W* s_out) {
+  constexpr int VW = 16 / sizeof(W);
+  constexpr int EE = E > 0 ? E : 1;
+  const unsigned long long cblk = local / it.vblocks;
+  const unsigned long long vblk = local - cblk * it.vblocks;
+  const int L = it.L;
+  const int g = threadIdx.x / L, lane = threadIdx.x - (threadIdx.x / L) * L;
+  const unsigned long long c0 = cblk * it.cb + (unsigned long long)g * kR;
+
+  W M[kR], K[kR], WX[kR][EE];
+  unsigned valid = 0;
+  Explicit<W> X;
+  if (E > 0) {
+#pragma unroll
+    for (int j = 0; j < EE; ++j) {
+      const Level& Lv = it.lv[it.inv + j];
+      X.kind[j] = Lv.kind;
+      X.op[j] = Lv.op;
+      X.sl[j] = Lv.small_left;
+      X.eps[j] = Lv.eps;
+      X.c[j] = (W)Lv.c;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kR; ++r) {
+    const unsigned long long c = c0 + r < it.nctx ? c0 + r : c0;  // pad with a duplicate
+    if (c0 + r < it.nctx) valid |= 1u << r;
+    W wl[kMaxDepth];
+    decode_context<W>(p, it, c, wl);
+    W m = (W)~W(0), k = p.target;
+    for (int l = 0; l < it.inv; ++l)
+      if (!invert_level<W>(it.lv[l], wl[l], m, k)) atomicOr(&p.flags[1], 1);
+    M[r] = m;
+    K[r] = k;
+    if (E > 0) {
+#pragma unroll
+      for (int j = 0; j < EE; ++j) WX[r][j] = wl[it.inv + j];
+    }
+  }
+
+  const W* V = p.tab[it.bottom];
+  const unsigned long long v0 = vblk * it.vb;
+  const unsigned long long v1 = umin64(v0 + it.vb, it.nv);
+  const unsigned long long q0 = v0 / VW, q1 = (v1 + VW - 1) / VW;
+  const uint4* V4 = reinterpret_cast<const uint4*>(V);
+
+  for (unsigned long long q = q0 + lane; q < q1; q += L) {
+    const uint4 raw = __ldg(V4 + q);
+    W xs[VW];
+    memcpy(xs, &raw, 16);
+    bool hit = false;
+#pragma unroll
+    for (int e = 0; e < VW; ++e) {
+#pragma unroll
+      for (int r = 0; r < kR; ++r) {
+        W y = xs[e];
+        if (E > 0) y = eval_explicit<W, E>(X, WX[r], y);
+        hit |= FULL ? (y == K[r]) : ((W)(y & M[r]) == K[r]);
+      }
+    }
+    if (hit) {
+#pragma unroll
+      for (int e = 0; e < VW; ++e) {
+        const unsigned long long v = q * VW + e;
+        if (v < v0 || v >= v1) continue;
+        for (int r = 0; r < kR; ++r) {
+          if (!(valid >> r & 1)) continue;
+          W y = xs[e];
+          if (E > 0) y = eval_explicit<W, E>(X, WX[r], y);
+          const bool h = FULL ? (y == K[r]) : ((W)(y & M[r]) == K[r]);
+          if (h) {
+            const unsigned long long rank = decode_context<W>(p, it, c0 + r, nullptr) + v * it.coefv;
+            push_hit<W>(p, sm, s_in, s_out, rank);
+          }
+        }
+      }
+    }
+  }
+}
+
+// Generic unit for spines with more than kMaxExplicit explicit levels:
+// straightforward bottom-up evaluation of every level, one context at a time.
+template <class W>
+__device__ void process_unit_generic(const Params<W>& p, Smem& sm, const Item& it,
+                                     unsigned long long local, const W* s_in, const W* s_out) {
+  const unsigned long long cblk = local / it.vblocks;
+  const unsigned long long vblk = local - cblk * it.vblocks;
+  const int L = it.L;
+  const int g = threadIdx.x / L, lane = threadIdx.x % L;
+  const unsigned long long v0 = vblk * it.vb;
+  const unsigned long long v1 = umin64(v0 + it.vb, it.nv);
+  const W* V = p.tab[it.bottom];
+  for (int r = 0; r < kR; ++r) {
+    const unsigned long long c = cblk * it.cb + (unsigned long long)g * kR + r;
+    if (c >= it.nctx) break;
+    W wl[kMaxDepth];
+    const unsigned long long rb = decode_context<W>(p, it, c, wl);
+    for (unsigned long long v = v0 + lane; v < v1; v += L) {
+      W y = V[v];
+      for (int l = it.depth - 1; l >= 0; --l) {
+        const Level& Lv = it.lv[l];
+        y = level_apply<W>(Lv.kind, Lv.op, Lv.small_left, Lv.eps, (W)Lv.c, wl[l], y);
+      }
+      if (y == p.target) push_hit<W>(p, sm, s_in, s_out, rb + v * it.coefv);
+    }
+  }
+}
+
+template <class W>
+__device__ void dispatch_unit(const Params<W>& p, Smem& sm, const Item& it, unsigned long long local,
+                              const W* s_in, const W* s_out) {
+  const int e = it.nexp;
+  if (e > kMaxExplicit) return process_unit_generic<W>(p, sm, it, local, s_in, s_out);
+  if (it.full) {
+    switch (e) {
+      case 0: return process_unit<W, 0, true>(p, sm, it, local, s_in, s_out);
+      case 1: return process_unit<W, 1, true>(p, sm, it, local, s_in, s_out);
+      case 2: return process_unit<W, 2, true>(p, sm, it, local, s_in, s_out);
+      case 3: return process_unit<W, 3, true>(p, sm, it, local, s_in, s_out);
+      default: return process_unit<W, 4, true>(p, sm, it, local, s_in, s_out);
+    }
+  }
+  switch (e) {
+    case 0: return process_unit<W, 0, false>(p, sm, it, local, s_in, s_out);
+    case 1: return process_unit<W, 1, false>(p, sm, it, local, s_in, s_out);
+    case 2: return process_unit<W, 2, false>(p, sm, it, local, s_in, s_out);
+    case 3: return process_unit<W, 3, false>(p, sm, it, local, s_in, s_out);
+    default: return process_unit<W, 4, false>(p, sm, it, local, s_in, s_out);
+  }
+}
+
+template <class W>
+__device__ void stage_samples(const Params<W>& p, Smem& sm, W* s_in, W* s_out) {
+  for (int i = threadIdx.x; i < (kMaxSize + 1) * kCols; i += blockDim.x) sm.counts[i] = p.counts[i];
+  // 16-byte vector copies; the device arrays are padded to 16 bytes.
+  const int nin = (p.S * p.K * (int)sizeof(W) + 15) / 16;
+  const int nout = (p.S * (int)sizeof(W) + 15) / 16;
+  const uint4* gi = reinterpret_cast<const uint4*>(p.in);
+  const uint4* go = reinterpret_cast<const uint4*>(p.out);
+  uint4* si = reinterpret_cast<uint4*>(s_in);
+  uint4* so = reinterpret_cast<uint4*>(s_out);
+  for (int i = threadIdx.x; i < nin; i += blockDim.x) si[i] = gi[i];
+  for (int i = threadIdx.x; i < nout; i += blockDim.x) so[i] = go[i];
+}
+
+// Persistent search kernel: CTAs take work units from an atomic counter.
+template <class W>
+__global__ void __launch_bounds__(kThreads) spine_kernel(Params<W> p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+  W* s_in = reinterpret_cast<W*>(smem_raw + ((sizeof(Smem) + 15) & ~size_t(15)));
+  W* s_out = s_in + ((p.S * p.K * (int)sizeof(W) + 15) / 16) * (16 / (int)sizeof(W));
+  stage_samples<W>(p, sm, s_in, s_out);
+  if (threadIdx.x == 0) {
+    sm.qn = 0;
+    sm.item_idx = -1;
+  }
+  __syncthreads();
+  for (;;) {
+    if (threadIdx.x == 0) {
+      unsigned long long u = atomicAdd(p.counter, 1ULL);
+      if (u >= p.total_units) u = ~0ULL;
+      if (u != ~0ULL && p.budget_ns && globaltimer_ns() - *p.start_ns > p.budget_ns) {
+        atomicOr(&p.flags[0], 1);
+        u = ~0ULL;
+      }
+      sm.unit = u;
+      if (u != ~0ULL) {
+        int lo = 0, hi = p.nitems - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (p.items[mid].unit_begin <= u) lo = mid;
+          else hi = mid - 1;
+        }
+        sm.next_item = lo;
+        sm.skip = p.stop_on_match && p.items[lo].base > *(volatile unsigned long long*)p.best;
+      }
+    }
+    __syncthreads();
+    const unsigned long long u = sm.unit;
+    if (u == ~0ULL) break;
+    const int ni = sm.next_item;
+    if (ni != sm.item_idx) {
+      const uint4* src = reinterpret_cast<const uint4*>(p.items + ni);
+      uint4* dst = reinterpret_cast<uint4*>(&sm.item);
+      for (int i = threadIdx.x; i < (int)(sizeof(Item) / 16); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    if (!sm.skip) {
+      const Item& it = sm.item;
+      const unsigned long long local = u - it.unit_begin;
+      dispatch_unit<W>(p, sm, it, local, s_in, s_out);
+      if (threadIdx.x == 0) {
+        const unsigned long long cblk = local / it.vblocks, vblk = local % it.vblocks;
+        const unsigned long long c0 = cblk * it.cb, c1 = umin64(c0 + it.cb, it.nctx);
+        const unsigned long long v0 = vblk * it.vb, v1 = umin64(v0 + it.vb, it.nv);
+        atomicAdd(p.evaluated, (c1 - c0) * (v1 - v0));
+      }
+    }
+    __syncthreads();
+    if (sm.qn > 0) verify_queue<W>(p, sm, s_in, s_out);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      sm.qn = 0;
+      sm.item_idx = ni;
+    }
+  }
+}
+
+// One thread per rank: unrank, evaluate sample 0, verify on a match.  This
+// is the reference's per-thread algorithm (nocache.cu:85-107) with the
+// count table and samples in shared memory, a grid-stride loop (no gridDim
+// overflow) and the minimum matching rank.
+template <class W>
+__global__ void __launch_bounds__(kThreads) naive_kernel(Params<W> p, unsigned long long lo,
+                                                         unsigned long long hi) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+  W* s_in = reinterpret_cast<W*>(smem_raw + ((sizeof(Smem) + 15) & ~size_t(15)));
+  W* s_out = s_in + ((p.S * p.K * (int)sizeof(W) + 15) / 16) * (16 / (int)sizeof(W));
+  stage_samples<W>(p, sm, s_in, s_out);
+  __syncthreads();
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  unsigned long long count = 0;
+  char post[kMaxSize + 1];
+  for (unsigned long long r = lo + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; r < hi;
+       r += stride) {
+    if (p.stop_on_match && r > *(volatile unsigned long long*)p.best) break;
+    if ((count & 1023) == 0 && p.budget_ns && globaltimer_ns() - *p.start_ns > p.budget_ns) {
+      atomicOr(&p.flags[0], 1);
+      break;
+    }
+    unrank(r, p.size, (const uint64_t(*)[kCols])sm.counts, post);
+    ++count;
+    if (eval_postfix<W>(post, p.size, s_in) != s_out[0]) continue;
+    bool ok = true;
+    for (int i = 1; i < p.S && ok; ++i) ok = eval_postfix<W>(post, p.size, s_in + i * p.K) == s_out[i];
+    if (ok) atomicMin(p.best, r);
+  }
+  atomicAdd(p.evaluated, count);
+}
+
+template <class W>
+__global__ void build_unary_kernel(W* out, const W* in, unsigned long long n, int op) {
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (unsigned long long)gridDim.x * blockDim.x)
+    out[i] = un_apply<W>(op, in[i]);
+}
+
+template <class W>
+__global__ void build_binary_kernel(W* out, const W* A, const W* B, unsigned long long na,
+                                    unsigned long long nb, int op) {
+  const unsigned long long n = na * nb;
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long a = i / nb;
+    out[i] = bin_apply<W>(op, A[a], B[i - a * nb]);
+  }
+}
+
+__global__ void stamp_start_kernel(unsigned long long* t) { *t = globaltimer_ns(); }
+
+// ------------------------------------------------------------------ host side
+
+struct ChainClass {
+  int eps;
+  int64_t c;
+  uint64_t off;
+};
+
+struct Enumerator {
+  const CountTable* ct;
+  int T;
+  uint64_t mask;
+  std::vector<Item>* items;
+  bool too_deep = false;
+
+  uint64_t N(int s) const { return ct->n[s][8]; }
+
+  void emit(int size, std::vector<Level>& lv, uint64_t mult, uint64_t base, const ChainClass& k) {
+    if (lv.size() + (k.eps == 1 && k.c == 0 ? 0 : 1) > (size_t)kMaxDepth) {
+      too_deep = true;
+      return;
+    }
+    Item it;
+    memset(&it, 0, sizeof(it));
+    int d = 0;
+    for (auto& L : lv) it.lv[d++] = L;
+    if (!(k.eps == 1 && k.c == 0)) {
+      Level L;
+      memset(&L, 0, sizeof(L));
+      L.kind = 1;
+      L.eps = (int8_t)k.eps;
+      L.c = (uint64_t)k.c & mask;
+      L.nsmall = 1;
+      it.lv[d++] = L;
+    }
+    it.depth = (int8_t)d;
+    it.bottom = (int8_t)size;
+    it.base = base + k.off;
+    it.coefv = mult;
+    it.nv = N(size);
+    items->push_back(it);
+  }
+
+  void rec(int size, std::vector<Level>& lv, uint64_t mult, uint64_t base,
+           const std::vector<ChainClass>& cls) {
+    if (too_deep) return;
+    if (size <= T) {
+      for (auto& k : cls) emit(size, lv, mult, base, k);
+      return;
+    }
+    if (lv.size() >= (size_t)kMaxDepth) {
+      too_deep = true;
+      return;
+    }
+    // Unary blocks: extend every chain class by ~ (x -> -x - 1) or neg
+    // (x -> -x), keeping the smallest rank offset per resulting map.
+    const uint64_t off_not = op_offset(ct->n, size, OP_NOT);
+    const uint64_t off_neg = op_offset(ct->n, size, OP_NEG);
+    std::vector<ChainClass> ncls;
+    auto add = [&](int eps, int64_t c, uint64_t off) {
+      for (auto& x : ncls)
+        if (x.eps == eps && x.c == c) {
+          x.off = std::min(x.off, off);
+          return;
+        }
+      ncls.push_back({eps, c, off});
+    };
+    for (auto& k : cls) {
+      add(-k.eps, k.c - k.eps, k.off + off_not * mult);
+      add(-k.eps, k.c, k.off + off_neg * mult);
+    }
+    rec(size - 1, lv, mult, base, ncls);
+    // Binary blocks in rank order.
+    const int sub = size - 1;
+    for (int op = 0; op < 8; ++op) {
+      if (is_unary(op)) continue;
+      uint64_t boff = op_offset(ct->n, size, op);
+      const int fmax = is_commutative(op) ? sub / 2 : sub - 1;
+      for (int f = 1; f <= fmax; ++f) {
+        const int i = f, j = sub - f;
+        for (auto& k : cls) {
+          std::vector<Level> lv2 = lv;
+          if (!(k.eps == 1 && k.c == 0)) {
+            Level C;
+            memset(&C, 0, sizeof(C));
+            C.kind = 1;
+            C.eps = (int8_t)k.eps;
+            C.c = (uint64_t)k.c & mask;
+            C.nsmall = 1;
+            lv2.push_back(C);
+          }
+          Level B;
+          memset(&B, 0, sizeof(B));
+          B.kind = 0;
+          B.op = (int8_t)op;
+          uint64_t nmult;
+          int big;
+          if (j >= i) {  // small = left operand
+            B.small_left = 1;
+            B.ts = (int8_t)i;
+            B.coef = mult * N(j);
+            nmult = mult;
+            big = j;
+          } else {  // small = right operand
+            B.small_left = 0;
+            B.ts = (int8_t)j;
+            B.coef = mult;
+            nmult = mult * N(j);
+            big = i;
+          }
+          B.nsmall = N(B.ts);
+          lv2.push_back(B);
+          if (lv2.size() > (size_t)kMaxDepth) {
+            too_deep = true;
+            return;
+          }
+          std::vector<ChainClass> id{{1, 0, 0}};
+          rec(big, lv2, nmult, base + k.off + boff * mult, id);
+        }
+        boff += N(i) * N(j);
+      }
+    }
+  }
+};
+
+// Structural inversion depth: levels are inverted top-down until the first
+// arithmetic level that lies below an & or | (its constraint mask is then
+// not of the form 2^n - 1).
+static void finish_item(Item& it, int threads, uint64_t mask) {
+  int inv = it.depth;
+  bool andor = false, full = true;
+  for (int l = 0; l < it.depth; ++l) {
+    const Level& L = it.lv[l];
+    const bool notchain = L.kind == 1 && L.eps < 0 && L.c == mask;  // the map x -> ~x
+    const bool arith = (L.kind == 0 && (L.op == OP_ADD || L.op == OP_SUB || L.op == OP_MUL)) ||
+                       (L.kind == 1 && !notchain);
+    if (andor && arith) {
+      inv = l;
+      break;
+    }
+    if (L.kind == 0 && (L.op == OP_AND || L.op == OP_OR)) {
+      andor = true;
+      full = false;
+    }
+    if (L.kind == 0 && L.op == OP_MUL) full = false;
+  }
+  it.inv = (int8_t)inv;
+  it.nexp = (int8_t)(it.depth - inv);
+  it.full = full ? 1 : 0;
+  uint64_t nctx = 1;
+  for (int l = 0; l < it.depth; ++l)
+    if (it.lv[l].kind == 0) nctx *= it.lv[l].nsmall;
+  it.nctx = nctx;
+  // thread layout: G groups of kR contexts, L lanes over the values
+  uint64_t groups = (nctx + kR - 1) / kR;
+  int G = 1;
+  while (G < threads && (uint64_t)G < groups) G <<= 1;
+  it.G = (uint16_t)G;
+  it.L = (uint16_t)(threads / G);
+  it.cb = (uint32_t)(G * kR);
+  it.cblocks = (nctx + it.cb - 1) / it.cb;
+  const uint64_t target = 1ULL << 22;  // candidates per unit
+  uint64_t vb = target / it.cb;
+  const uint64_t align = 64ULL * it.L;
+  vb = std::max<uint64_t>(align, (vb + align - 1) / align * align);
+  const uint64_t nv_al = (it.nv + 63) / 64 * 64;
+  if (vb > nv_al) vb = nv_al;
+  it.vb = vb;
+  it.vblocks = (it.nv + vb - 1) / vb;
+}
+
+template <class W>
+class Search final : public SearchSession {
+ public:
+  Search(const HostInstance& h, const EngineOptions& o) : h_(h), o_(o) {}
+  ~Search() override {
+    if (stream_ && own_stream_) cudaStreamDestroy(stream_);
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (evk_) cudaEventDestroy(evk_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    if (h_scal_) cudaFreeHost(h_scal_);
+  }
+
+  int init() {
+    SB_CUDA(cudaSetDevice(o_.device));
+    if (o_.stream) {
+      stream_ = reinterpret_cast<cudaStream_t>(o_.stream);
+      own_stream_ = false;
+    } else {
+      SB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+      own_stream_ = true;
+    }
+    SB_CUDA(cudaEventCreate(&ev0_));
+    SB_CUDA(cudaEventCreate(&evk_));
+    SB_CUDA(cudaEventCreate(&ev1_));
+    SB_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, o_.device));
+    mask_ = h_.bits == 64 ? ~0ULL : 0xFFFFFFFFULL;
+    // count table up to the largest size whose counts fit in 64 bits
+    CountTable t;
+    int ms = kMaxSize;
+    while (ms > 1 && !build_count_table(ms, h_.k, &t)) --ms;
+    build_count_table(ms, h_.k, &ct_);
+    count_ok_max_ = ms;
+    // samples as W words, padded to 16 bytes
+    const size_t nin = (size_t)h_.S * h_.k, nout = (size_t)h_.S;
+    std::vector<W> win((nin * sizeof(W) + 15) / 16 * 16 / sizeof(W), 0);
+    std::vector<W> wout((nout * sizeof(W) + 15) / 16 * 16 / sizeof(W), 0);
+    for (size_t i = 0; i < nin; ++i) win[i] = (W)h_.in[i];
+    for (size_t i = 0; i < nout; ++i) wout[i] = (W)h_.out[i];
+    SB_CUDA(d_in_.reserve(win.size() * sizeof(W)));
+    SB_CUDA(d_out_.reserve(wout.size() * sizeof(W)));
+    SB_CUDA(cudaMemcpy(d_in_.p, win.data(), win.size() * sizeof(W), cudaMemcpyHostToDevice));
+    SB_CUDA(cudaMemcpy(d_out_.p, wout.data(), wout.size() * sizeof(W), cudaMemcpyHostToDevice));
+    SB_CUDA(d_counts_.reserve(sizeof(ct_.n)));
+    SB_CUDA(cudaMemcpy(d_counts_.p, ct_.n, sizeof(ct_.n), cudaMemcpyHostToDevice));
+    SB_CUDA(d_scal_.reserve(256));
+    SB_CUDA(cudaHostAlloc(&h_scal_, 256, cudaHostAllocDefault));
+    // table budget -> largest tabled size
+    const int64_t budget = o_.table_bytes > 0 ? o_.table_bytes : (4LL << 30);
+    uint64_t total = 0;
+    Tcap_ = 0;
+    for (int t = 1; t <= count_ok_max_ && t <= 20; ++t) {
+      const uint64_t bytes = padded(ct_.n[t][8]) * sizeof(W);
+      if (total + bytes > (uint64_t)budget) break;
+      total += bytes;
+      Tcap_ = t;
+    }
+    if (Tcap_ < 1) Tcap_ = 1;
+    SB_CUDA(d_tab_.reserve(total + 256));
+    uint64_t off = 0;
+    for (int t = 1; t <= Tcap_; ++t) {
+      tab_off_[t] = off;
+      off += padded(ct_.n[t][8]) * sizeof(W);
+    }
+    built_ = 0;
+    smem_bytes_ = ((sizeof(Smem) + 15) & ~size_t(15)) +
+                  (((size_t)h_.S * h_.k * sizeof(W) + 15) / 16 + ((size_t)h_.S * sizeof(W) + 15) / 16) * 16;
+    SB_CUDA(cudaFuncSetAttribute(spine_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem_bytes_));
+    SB_CUDA(cudaFuncSetAttribute(naive_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem_bytes_));
+    int occ = 1;
+    SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, spine_kernel<W>, kThreads, smem_bytes_));
+    grid_ = sms_ * std::max(occ, 1);
+    int occn = 1;
+    SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occn, naive_kernel<W>, kThreads, smem_bytes_));
+    grid_naive_ = sms_ * std::max(occn, 1);
+    return 0;
+  }
+
+  int solve(int max_size, SolveOutcome* out) override { return run(max_size, 0, 0, true, out); }
+  int sweep(int lo, int hi, SolveOutcome* out) override { return run(hi, lo, hi, false, out); }
+
+ private:
+  static uint64_t padded(uint64_t n) { return (n + 63) / 64 * 64 + 64; }
+
+  W* tab(int t) const { return reinterpret_cast<W*>(d_tab_.as<char>() + tab_off_[t]); }
+
+  // Build V_{built+1} .. V_t (each entry one operator over smaller tables).
+  int ensure_tables(int t) {
+    for (int s = built_ + 1; s <= t; ++s) {
+      W* o = tab(s);
+      if (s == 1) {
+        std::vector<W> v(padded(h_.k), 0);
+        for (int j = 0; j < h_.k; ++j) v[j] = (W)h_.in[j];
+        SB_CUDA(cudaMemcpyAsync(o, v.data(), v.size() * sizeof(W), cudaMemcpyHostToDevice, stream_));
+      } else {
+        uint64_t off = 0;
+        const int sub = s - 1;
+        for (int op = 0; op < 8; ++op) {
+          if (is_unary(op)) {
+            const uint64_t n = ct_.n[sub][8];
+            const int blocks = (int)std::min<uint64_t>((n + 255) / 256, (uint64_t)sms_ * 16);
+            build_unary_kernel<W><<<blocks, 256, 0, stream_>>>(o + off, tab(sub), n, op);
+            ++launches_;
+            off += n;
+            continue;
+          }
+          const int fmax = is_commutative(op) ? sub / 2 : sub - 1;
+          for (int f = 1; f <= fmax; ++f) {
+            const uint64_t na = ct_.n[f][8], nb = ct_.n[sub - f][8];
+            const uint64_t n = na * nb;
+            const int blocks = (int)std::min<uint64_t>((n + 255) / 256, (uint64_t)sms_ * 16);
+            build_binary_kernel<W><<<blocks, 256, 0, stream_>>>(o + off, tab(f), tab(sub - f), na, nb, op);
+            ++launches_;
+            off += n;
+          }
+        }
+      }
+      SB_CUDA(cudaGetLastError());
+      built_ = s;
+    }
+    return 0;
+  }
+
+  Params<W> params(int s) {
+    Params<W> p;
+    memset(&p, 0, sizeof(p));
+    for (int t = 1; t <= built_; ++t) p.tab[t] = tab(t);
+    p.in = d_in_.as<W>();
+    p.out = d_out_.as<W>();
+    p.counts = d_counts_.as<unsigned long long>();
+    unsigned long long* sc = d_scal_.as<unsigned long long>();
+    p.counter = sc + 0;
+    p.best = sc + 1;
+    p.evaluated = sc + 2;
+    p.start_ns = sc + 3;
+    p.flags = reinterpret_cast<int*>(sc + 4);
+    p.target = (W)h_.out[0];
+    p.size = s;
+    p.S = h_.S;
+    p.K = h_.k;
+    p.budget_ns = o_.budget_s > 0 ? (unsigned long long)(o_.budget_s * 1e9) : 0;
+    return p;
+  }
+
+  // Search one size; writes the minimum matching rank (or ~0) and the number
+  // of candidates evaluated.  status: 0 ok, SIMBA_BUDGET on budget expiry.
+  // Integer lane-operations per candidate that the algorithm needs: the
+  // masked compare of the bottom value plus every explicitly evaluated level
+  // (64-bit words take two 32-bit lane operations per bitwise or add/sub
+  // step and three per multiply).
+  static double alg_cost(const Item& it) {
+    const double w = sizeof(W) == 8 ? 2.0 : 1.0;
+    double c = it.full ? w : w + 1.0;
+    for (int l = it.inv; l < it.depth; ++l) {
+      const Level& L = it.lv[l];
+      c += (L.kind == 0 && L.op == OP_MUL) ? (sizeof(W) == 8 ? 3.0 : 1.0) : w;
+    }
+    return c;
+  }
+
+  int search_size(int s, bool stop, uint64_t* best, uint64_t* evaluated, double* ms) {
+    double alg_total = 0;
+    // reset counter, best, evaluated, flags
+    unsigned long long init[8] = {0, ~0ULL, 0, 0, 0, 0, 0, 0};
+    SB_CUDA(cudaMemcpyAsync(d_scal_.p, init, 3 * sizeof(unsigned long long), cudaMemcpyHostToDevice, stream_));
+    SB_CUDA(cudaMemsetAsync(d_scal_.as<unsigned long long>() + 4, 0, 4 * sizeof(unsigned long long), stream_));
+    const bool spine_ok = o_.engine == 0 && s <= count_ok_max_;
+    int T = std::min(Tcap_, s);
+    bool use_naive = !spine_ok || (s > T && (s - 1) / 2 > T);
+    std::vector<Item> items;
+    if (!use_naive) {
+      if (s <= T) {
+        Item it;
+        memset(&it, 0, sizeof(it));
+        it.depth = 0;
+        it.bottom = (int8_t)s;
+        it.base = 0;
+        it.coefv = 1;
+        it.nv = ct_.n[s][8];
+        items.push_back(it);
+      } else {
+        Enumerator en;
+        en.ct = &ct_;
+        en.T = T;
+        en.mask = mask_;
+        en.items = &items;
+        std::vector<Level> lv;
+        std::vector<ChainClass> top{{1, 0, 0}};
+        en.rec(s, lv, 1, 0, top);
+        if (en.too_deep) use_naive = true;
+      }
+    }
+    SB_CUDA(cudaEventRecord(ev0_, stream_));
+    if (!use_naive) {
+      int rc = ensure_tables(std::min(T, s));
+      if (rc) return rc;
+      uint64_t units = 0;
+      for (auto& it : items) {
+        for (int l = 0; l < it.depth; ++l)
+          if (it.lv[l].kind == 1) it.lv[l].c &= mask_;
+        finish_item(it, kThreads, mask_);
+        it.unit_begin = units;
+        units += it.cblocks * it.vblocks;
+      }
+      SB_CUDA(d_items_.reserve(items.size() * sizeof(Item)));
+      SB_CUDA(cudaMemcpyAsync(d_items_.p, items.data(), items.size() * sizeof(Item),
+                              cudaMemcpyHostToDevice, stream_));
+      for (auto& it : items) alg_total += (double)it.nctx * (double)it.nv * alg_cost(it);
+      Params<W> p = params(s);
+      p.items = d_items_.as<Item>();
+      p.nitems = (int)items.size();
+      p.total_units = units;
+      p.stop_on_match = stop ? 1 : 0;
+      SB_CUDA(cudaEventRecord(evk_, stream_));
+      spine_kernel<W><<<grid_, kThreads, smem_bytes_, stream_>>>(p);
+      ++launches_;
+      SB_CUDA(cudaGetLastError());
+    } else {
+      Params<W> p = params(s);
+      p.stop_on_match = stop ? 1 : 0;
+      alg_total = (double)ct_.n[s][8] * (double)s * (sizeof(W) == 8 ? 2.0 : 1.0);
+      SB_CUDA(cudaEventRecord(evk_, stream_));
+      naive_kernel<W><<<grid_naive_, kThreads, smem_bytes_, stream_>>>(p, 0, ct_.n[s][8]);
+      ++launches_;
+      SB_CUDA(cudaGetLastError());
+    }
+    SB_CUDA(cudaEventRecord(ev1_, stream_));
+    SB_CUDA(cudaMemcpyAsync(h_scal_, d_scal_.p, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_));
+    SB_CUDA(cudaStreamSynchronize(stream_));
+    float e = 0, ek = 0;
+    SB_CUDA(cudaEventElapsedTime(&e, ev0_, ev1_));
+    SB_CUDA(cudaEventElapsedTime(&ek, evk_, ev1_));
+    *ms += e;
+    kernel_ms_ += ek;
+    const unsigned long long* hs = static_cast<unsigned long long*>(h_scal_);
+    *best = hs[1];
+    *evaluated += hs[2];
+    const double cand_total = use_naive ? (double)ct_.n[s][8] : [&] {
+      double c = 0;
+      for (auto& it : items) c += (double)it.nctx * (double)it.nv;
+      return c;
+    }();
+    if (cand_total > 0) alg_ops_ += (uint64_t)(alg_total * ((double)hs[2] / cand_total));
+    const int* fl = reinterpret_cast<const int*>(hs + 4);
+    last_T_ = use_naive ? 0 : T;
+    if (fl[1]) {
+      set_last_error("inversion failed on a level marked invertible");
+      return SIMBA_E_INTERNAL;
+    }
+    if (o_.verbose)
+      fprintf(stderr, "size %2d | %s | items %zu | evaluated %llu | %.3f ms\n", s,
+              use_naive ? "naive" : "spine", items.size(), (unsigned long long)hs[2], e);
+    return fl[0] ? SIMBA_BUDGET : 0;
+  }
+
+  int run(int max_size, int lo, int hi, bool stop, SolveOutcome* out) {
+    *out = SolveOutcome();
+    int first, last;
+    if (stop) {
+      first = o_.size_range ? 1 : 2;
+      last = o_.size_range ? max_size : max_size - 1;
+    } else {
+      first = lo;
+      last = hi;
+    }
+    if (last > count_ok_max_) {
+      set_last_error("candidate counts exceed 64 bits at this size");
+      return SIMBA_E_OVERFLOW;
+    }
+    launches_ = 0;
+    kernel_ms_ = 0.0;
+    alg_ops_ = 0;
+    stamp_start_kernel<<<1, 1, 0, stream_>>>(d_scal_.as<unsigned long long>() + 3);
+    ++launches_;
+    SB_CUDA(cudaGetLastError());
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int s = first; s <= last; ++s) {
+      if (o_.budget_s > 0) {
+        const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > o_.budget_s) {
+          out->status = SIMBA_BUDGET;
+          return SIMBA_BUDGET;
+        }
+      }
+      uint64_t best = ~0ULL;
+      int rc = search_size(s, stop, &best, &out->evaluated, &out->device_ms);
+      out->launches = launches_;
+      out->kernel_ms = kernel_ms_;
+      out->alg_ops = alg_ops_;
+      out->max_size_searched = s;
+      out->table_size = std::max(out->table_size, last_T_);
+      if (rc == SIMBA_BUDGET) {
+        out->status = SIMBA_BUDGET;
+        return SIMBA_BUDGET;
+      }
+      if (rc) return rc;
+      if (best != ~0ULL && stop) {
+        const int op = s == 1 ? 8 : op_of_rank(ct_.n, s, best);
+        uint64_t c = 0;
+        if (s == 1) c = best + 1;
+        else
+          for (int q = 0; q <= op; ++q) c += ct_.n[s][q];
+        out->per_size[s] = c;
+        out->candidates += c;
+        char buf[kMaxSize + 1];
+        unrank(best, s, ct_.n, buf);
+        buf[s] = 0;
+        out->postfix = buf;
+        out->size = s;
+        out->op = op;
+        out->rank = best;
+        if (!host_check(out->postfix, h_)) {
+          set_last_error("device match failed the host re-check");
+          return SIMBA_E_INTERNAL;
+        }
+        out->status = SIMBA_OK;
+        return SIMBA_OK;
+      }
+      out->per_size[s] = ct_.n[s][8];
+      out->candidates += ct_.n[s][8];
+      if (!stop && best != ~0ULL && out->status != SIMBA_OK) {
+        // sweeps report the first size with a match but keep going
+        char buf[kMaxSize + 1];
+        unrank(best, s, ct_.n, buf);
+        buf[s] = 0;
+        out->postfix = buf;
+        out->size = s;
+        out->op = s == 1 ? 8 : op_of_rank(ct_.n, s, best);
+        out->rank = best;
+        out->status = SIMBA_OK;
+      }
+    }
+    if (out->status != SIMBA_OK) out->status = SIMBA_NOT_FOUND;
+    return out->status;
+  }
+
+  HostInstance h_;
+  EngineOptions o_;
+  CountTable ct_;
+  int count_ok_max_ = 0;
+  uint64_t mask_ = 0;
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, evk_ = nullptr, ev1_ = nullptr;
+  bool own_stream_ = true;
+  int launches_ = 0;
+  double kernel_ms_ = 0.0;
+  uint64_t alg_ops_ = 0;
+  int sms_ = 0, grid_ = 0, grid_naive_ = 0;
+  size_t smem_bytes_ = 0;
+  DevBuf d_in_, d_out_, d_counts_, d_scal_, d_tab_, d_items_;
+  void* h_scal_ = nullptr;
+  uint64_t tab_off_[kMaxSize + 1] = {};
+  int Tcap_ = 0, built_ = 0, last_T_ = 0;
+};
+
+int make_search_session(const HostInstance& h, const EngineOptions& o, SearchSession** out) {
+  *out = nullptr;
+  int rc = validate(h, 1);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= o.device || o.device < 0) {
+    cudaGetLastError();
+    set_last_error("no usable CUDA device");
+    return SIMBA_E_NODEV;
+  }
+  if (h.bits == 64) {
+    auto s = std::make_unique<Search<uint64_t>>(h, o);
+    rc = s->init();
+    if (rc) return rc;
+    *out = s.release();
+  } else {
+    auto s = std::make_unique<Search<uint32_t>>(h, o);
+    rc = s->init();
+    if (rc) return rc;
+    *out = s.release();
+  }
+  return 0;
+}
+
+}  // namespace simba

@@ -1,0 +1,160 @@
+"""The CPU oracle, pinned against the reference's own outputs (no GPU needed).
+
+Pins:
+  * ref_instances_u32.json: formulas and uint32 outputs produced by the
+    reference's scripts/generate.py + scripts/sample.py;
+  * ref_results_u32.json: answers printed by the reference executables
+    (simba/src/nocache.cu, vfb/src/full-cache.cu rebuilt for sm_100a) on
+    those instances;
+  * the rank-space sizes the reference's count table implies.
+"""
+import numpy as np
+import pytest
+
+from simba_b200.instances import (Instance, eval_postfix, infix_to_postfix, make_instance,
+                                  postfix_to_infix)
+
+OPS = "~&|^#+-*"
+
+
+def test_count_table_recurrence(oracle):
+    t = oracle.count_table(8, 2)
+    assert list(t[1]) == [0] * 8 + [2]
+    assert list(t[2]) == [2, 0, 0, 0, 2, 0, 0, 0, 4]
+    assert list(t[3]) == [4] * 8 + [32]
+    assert [int(t[s][8]) for s in range(2, 8)] == [4, 32, 120, 784, 4144, 28768]
+
+
+def test_count_table_overflow_detected(oracle):
+    with pytest.raises(OverflowError):
+        oracle.count_table(22, 6)
+
+
+@pytest.mark.parametrize("k,size", [(1, 5), (2, 6), (3, 5)])
+def test_unrank_is_a_bijection(oracle, k, size):
+    t = oracle.count_table(size, k)
+    n = int(t[size][8])
+    seen = {oracle.unrank(r, size, t) for r in range(n)}
+    assert len(seen) == n
+    for p in seen:  # every string is a well-formed tree of `size` nodes
+        depth = 0
+        for c in p:
+            if c in "~#":
+                assert depth >= 1
+            elif c in OPS:
+                depth -= 1
+            else:
+                depth += 1
+        assert depth == 1
+
+
+def test_unrank_block_structure(oracle):
+    """Ranks are op-major in the order ~ & | ^ neg + - *; commutative splits
+    have left size <= right size (simba/src/nocache.cu:53-79, 137-144)."""
+    k, s = 2, 6
+    t = oracle.count_table(s, k)
+    off = 0
+    for op in range(8):
+        n = int(t[s][op])
+        for r in (off, off + n - 1):
+            assert oracle.unrank(r, s, t)[-1] == OPS[op]
+        off += n
+
+
+def test_golden_formulas_evaluate(oracle, golden):
+    for d in golden["instances"]:
+        inst = Instance.from_json(d)
+        p = infix_to_postfix(d["original_formula"])
+        assert postfix_to_infix(p) == d["original_formula"]
+        assert oracle.check(p, inst.inputs, inst.outputs, 32)
+        ev = eval_postfix(p, inst.inputs.astype(np.uint32), 32).astype(np.uint64)
+        assert (ev == inst.outputs).all()
+
+
+def test_oracle_matches_reference_simba(oracle, golden):
+    """Same size and same root-operator block as the reference executable;
+    identical string whenever the reference's block has a single match."""
+    same_string = 0
+    for r in golden["results"]["simba"]:
+        d = golden["instances"][r["idx"]]
+        inst = Instance.from_json(d)
+        o = oracle.search(inst.inputs, inst.outputs, r["max_len"], 32)
+        if r["expr"] == "Not found !":
+            assert not o["found"]
+            continue
+        p = infix_to_postfix(r["expr"])
+        assert oracle.check(p, inst.inputs, inst.outputs, 32)
+        assert o["found"] and len(p) == o["size"]
+        assert OPS.index(p[-1]) == o["op"]
+        if p == o["postfix"]:
+            same_string += 1
+        else:
+            # a multi-match block: the reference returns a racy winner, the
+            # oracle the minimum rank; both must be matches of that block
+            t = oracle.count_table(o["size"], inst.num_variables)
+            lo = int(sum(int(x) for x in t[o["size"]][: o["op"]]))
+            hi = lo + int(t[o["size"]][o["op"]])
+            e, mr, nh = oracle.scan_range(inst.inputs, inst.outputs, o["size"], lo, hi, 32)
+            assert mr == o["rank"]
+    assert same_string >= 100
+
+
+def test_oracle_matches_reference_vfb(oracle, golden):
+    """The reference VFB (with its uniqueness test as written) is emulated
+    exactly: found / not found and size agree on every golden instance."""
+    for r in golden["results"]["vfb"]:
+        d = golden["instances"][r["idx"]]
+        inst = Instance.from_json(d)
+        o = oracle.vfb(inst.inputs, inst.outputs, r["max_len"], 32, ref_inverted=True)
+        if r["expr"] in ("Not found !", ""):
+            assert not o["found"]
+            continue
+        p = infix_to_postfix(r["expr"])
+        assert oracle.check(p, inst.inputs, inst.outputs, 32)
+        assert o["found"] and o["size"] == len(p)
+
+
+def test_vfb_correct_dedup_is_minimal(oracle):
+    """With the documented dedup (keep first occurrence) VFB finds the same
+    minimal size as the exhaustive plain search."""
+    for seed in range(6):
+        inst = make_instance(7, 2, 16, seed, word_bits=64)
+        v = oracle.vfb(inst.inputs, inst.outputs, 8, 64)
+        s = oracle.search(inst.inputs, inst.outputs, 9, 64, include_edges=True)
+        assert v["found"] == s["found"]
+        if s["found"]:
+            assert v["size"] == s["size"]
+            assert oracle.check(v["postfix"], inst.inputs, inst.outputs, 64)
+
+
+def test_reference_vfb_inverted_dedup_differs():
+    """Documented finding: the reference's `insert(...) > 0` keeps repeated
+    vectors; on the size-9 two-variable instance it answers one size later."""
+    from oracle import oracle as O
+    inst = make_instance(9, 2, 32, 0, word_bits=64)
+    a = O.vfb(inst.inputs, inst.outputs, 12, 64, ref_inverted=False)
+    b = O.vfb(inst.inputs, inst.outputs, 12, 64, ref_inverted=True)
+    assert a["size"] == 5 and b["size"] == 6
+
+
+def test_fingerprint32_properties(oracle):
+    v = np.arange(16, dtype=np.uint32)
+    f = oracle.fingerprint32(v)
+    assert f == oracle.fingerprint32(v.copy())
+    v2 = v.copy()
+    v2[3] ^= 1
+    assert f != oracle.fingerprint32(v2)
+
+
+def test_u64_wraparound(oracle):
+    row = np.array([2 ** 63 + 5, 2 ** 64 - 1], dtype=np.uint64)
+    assert oracle.eval1("01+", row, 64) == (2 ** 63 + 5 + 2 ** 64 - 1) % 2 ** 64
+    assert oracle.eval1("01*", row, 64) == ((2 ** 63 + 5) * (2 ** 64 - 1)) % 2 ** 64
+    assert oracle.eval1("0#", row, 64) == (2 ** 64 - (2 ** 63 + 5)) % 2 ** 64
+    assert oracle.eval1("01*", row, 32) == ((5) * (2 ** 32 - 1)) % 2 ** 32
+
+
+def test_scan_range_counts(oracle):
+    inst = make_instance(9, 2, 32, 3, word_bits=64, unsat=True)
+    e, mr, nh = oracle.scan_range(inst.inputs, inst.outputs, 6, 0, 5000, 64)
+    assert e == 5000 and nh == 0 and mr == 2 ** 64 - 1
