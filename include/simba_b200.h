@@ -56,7 +56,11 @@ typedef struct {
   double budget_seconds; /* 0 = unlimited                                        */
   int64_t table_bytes;   /* cap on the value tables, 0 = default (4 GiB)         */
   uint64_t stream;       /* cudaStream_t to launch on (0 = library-owned stream)  */
-  int32_t reserved[6];
+  int64_t vfb_cache_rows;/* VFB row capacity, 0 = the reference's rule
+                            (max pitch / (4 * samples), full-cache.cu:713-718)  */
+  int32_t vfb_reference_dedup; /* 1: VFB keeps the reference's uniqueness test
+                            as written (stores repeated vectors)                */
+  int32_t reserved[3];
 } simba_options;
 
 typedef struct {
@@ -86,6 +90,33 @@ typedef struct {
  * Returns result.status. */
 int simba_solve(const simba_instance *inst, int max_size, const simba_options *opt,
                 simba_result *result);
+
+/* VFB bottom-up search result. */
+typedef struct {
+  int32_t status;
+  int32_t size;
+  int32_t op;            /* operator block of the answer, 8 = a variable         */
+  int32_t max_size_searched;
+  char postfix[256];
+  char expr[2048];       /* VFB syntax, e.g. (v0)+(~(v1)) (full-cache.cu:483-509) */
+  double seconds;
+  double device_ms;
+  uint64_t candidates;   /* allMBAs as the reference counts it                   */
+  int64_t rows_total;    /* cached characteristic vectors                        */
+  int64_t rows_per_size[101];
+  uint64_t cache_bytes;  /* bytes of the row cache                               */
+  uint64_t table_bytes;  /* bytes of the dedup hash table                        */
+  double bytes_moved;    /* algorithmic HBM bytes of the composition kernels     */
+  int32_t launches;
+  int32_t reserved;
+} vfb_result;
+
+/* VFB bottom-up enumeration with observational-equivalence dedup: replaces
+ * MBA() / generateMBAs (vfb/src/full-cache.cu:568-774).  Sizes 1..max_len,
+ * operators ~ & | ^ neg + - *, stop after the operator block that produces
+ * the target; "Not found !" when max_len is reached or the cache fills. */
+int vfb_solve(const simba_instance *inst, int max_len, const simba_options *opt,
+              vfb_result *result);
 
 /* Resident session: samples and value tables stay on the device between
  * calls (used by the benchmark to time the search with inputs in HBM). */

@@ -42,7 +42,18 @@ class _Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("size_range", C.c_int32), ("verbose", C.c_int32),
                 ("engine", C.c_int32), ("budget_seconds", C.c_double),
                 ("table_bytes", C.c_int64), ("stream", C.c_uint64),
-                ("reserved", C.c_int32 * 6)]
+                ("vfb_cache_rows", C.c_int64), ("vfb_reference_dedup", C.c_int32),
+                ("reserved", C.c_int32 * 3)]
+
+
+class _VfbResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("size", C.c_int32), ("op", C.c_int32),
+                ("max_size_searched", C.c_int32), ("postfix", C.c_char * 256),
+                ("expr", C.c_char * 2048), ("seconds", C.c_double), ("device_ms", C.c_double),
+                ("candidates", C.c_uint64), ("rows_total", C.c_int64),
+                ("rows_per_size", C.c_int64 * 101), ("cache_bytes", C.c_uint64),
+                ("table_bytes", C.c_uint64), ("bytes_moved", C.c_double),
+                ("launches", C.c_int32), ("reserved", C.c_int32)]
 
 
 class _Result(C.Structure):
@@ -84,6 +95,7 @@ def lib():
     L.simba_status_string.argtypes = [C.c_int]
     L.simba_device_count.restype = C.c_int
     L.simba_int_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    L.vfb_solve.argtypes = [P(_Instance), C.c_int, P(_Options), P(_VfbResult)]
     _lib = L
     return L
 
@@ -130,7 +142,7 @@ class _Arrays:
 
 
 def _opts(device=0, complete=False, verbose=False, naive=False, budget=0.0,
-          table_bytes=0, stream=0) -> _Options:
+          table_bytes=0, stream=0, cache_rows=0, reference_dedup=False) -> _Options:
     o = _Options()
     o.device = device
     o.size_range = 1 if complete else 0
@@ -139,6 +151,8 @@ def _opts(device=0, complete=False, verbose=False, naive=False, budget=0.0,
     o.budget_seconds = float(budget)
     o.table_bytes = int(table_bytes)
     o.stream = int(stream)
+    o.vfb_cache_rows = int(cache_rows)
+    o.vfb_reference_dedup = 1 if reference_dedup else 0
     return o
 
 
@@ -155,6 +169,41 @@ def solve(inst: Instance, max_size: int, **kw) -> Result:
     rc = lib().simba_solve(C.byref(a.c), max_size, C.byref(_opts(**kw)), C.byref(r))
     _check(rc)
     return _res(r)
+
+
+@dataclass
+class VfbResult:
+    status: int
+    size: int = 0
+    op: int = -1
+    postfix: str = ""
+    expr: str = "Not found !"
+    seconds: float = 0.0
+    device_ms: float = 0.0
+    candidates: int = 0
+    rows_total: int = 0
+    rows_per_size: List[int] = field(default_factory=list)
+    cache_bytes: int = 0
+    table_bytes: int = 0
+    bytes_moved: float = 0.0
+    launches: int = 0
+    max_size_searched: int = 0
+
+    @property
+    def found(self) -> bool:
+        return self.status == OK
+
+
+def vfb_solve(inst: Instance, max_len: int, **kw) -> VfbResult:
+    """VFB bottom-up search (the reference's MBA(), vfb/src/full-cache.cu:665-774)."""
+    a = _Arrays(inst)
+    r = _VfbResult()
+    rc = lib().vfb_solve(C.byref(a.c), max_len, C.byref(_opts(**kw)), C.byref(r))
+    _check(rc)
+    return VfbResult(r.status, r.size, r.op, r.postfix.decode(), r.expr.decode(), r.seconds,
+                     r.device_ms, r.candidates, r.rows_total, list(r.rows_per_size),
+                     r.cache_bytes, r.table_bytes, r.bytes_moved, r.launches,
+                     r.max_size_searched)
 
 
 class Session:

@@ -322,6 +322,47 @@ int simba_session_sweep(simba_session* session, int lo, int hi, simba_result* re
   return result->status;
 }
 
+int vfb_solve(const simba_instance* inst, int max_len, const simba_options* opt, vfb_result* result) {
+  if (!result) return SIMBA_E_ARG;
+  memset(result, 0, sizeof(*result));
+  const auto t0 = std::chrono::steady_clock::now();
+  HostInstance h;
+  int rc = to_host(inst, &h);
+  if (rc) {
+    result->status = rc;
+    return rc;
+  }
+  VfbOutcome oc;
+  rc = vfb_run(h, max_len, to_opts(opt), opt ? opt->vfb_reference_dedup : 0,
+               opt ? opt->vfb_cache_rows : 0, &oc);
+  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (rc < 0) {
+    result->status = rc;
+    return rc;
+  }
+  result->status = oc.status;
+  result->size = oc.size;
+  result->op = oc.op;
+  result->max_size_searched = oc.max_size_searched;
+  snprintf(result->postfix, sizeof(result->postfix), "%s", oc.postfix.c_str());
+  if (oc.status == SIMBA_OK) {
+    const std::string e = format_postfix(oc.postfix, 1);
+    snprintf(result->expr, sizeof(result->expr), "%s", e.c_str());
+  } else {
+    snprintf(result->expr, sizeof(result->expr), "Not found !");
+  }
+  result->seconds = secs;
+  result->device_ms = oc.device_ms;
+  result->candidates = oc.candidates;
+  result->rows_total = oc.rows_total;
+  for (int i = 0; i <= 100; ++i) result->rows_per_size[i] = oc.rows_per_size[i];
+  result->cache_bytes = oc.cache_bytes;
+  result->table_bytes = oc.table_bytes;
+  result->bytes_moved = oc.bytes_moved;
+  result->launches = oc.launches;
+  return result->status;
+}
+
 void simba_session_destroy(simba_session* session) {
   if (!session) return;
   delete session->s;

@@ -74,6 +74,27 @@ int read_instance_json(const std::string& path, HostInstance* h);
 
 int measure_int_peak(int device, double* lane_ops_per_s);
 
+struct VfbOutcome {
+  int status = SIMBA_NOT_FOUND;
+  int size = 0;
+  int op = -1;
+  std::string postfix;
+  double device_ms = 0.0;
+  uint64_t candidates = 0;
+  int64_t rows_total = 0;
+  int64_t rows_per_size[101] = {};
+  uint64_t cache_bytes = 0;
+  uint64_t table_bytes = 0;
+  double bytes_moved = 0.0;
+  int launches = 0;
+  int max_size_searched = 0;
+};
+
+// VFB bottom-up search (vfb.cu).  inverted = 1 keeps the reference's
+// uniqueness test as written; cache_rows = 0 uses the reference capacity.
+int vfb_run(const HostInstance& h, int max_len, const EngineOptions& o, int inverted,
+            int64_t cache_rows, VfbOutcome* out);
+
 // Format a postfix string in the SIMBA (style 0) or VFB (style 1) syntax.
 std::string format_postfix(const std::string& postfix, int style);
 

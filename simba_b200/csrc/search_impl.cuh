@@ -34,11 +34,13 @@
 //    verified by a whole warp: each lane evaluates different samples (staged
 //    in shared memory) and a ballot rejects the candidate at the first
 //    mismatching group of samples.
+#pragma once
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
+#include <cstddef>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -68,7 +70,7 @@ struct Level {
   int8_t pad[3];
 };
 
-struct Item {
+struct alignas(16) Item {
   uint64_t base;        // rank of the all-zero indices
   uint64_t coefv;       // rank coefficient of the bottom index
   uint64_t nctx;        // number of contexts
@@ -106,9 +108,9 @@ struct Params {
   int stop_on_match;
 };
 
-struct Smem {
+struct alignas(16) Smem {
   unsigned long long counts[(kMaxSize + 1) * kCols];
-  Item item;
+  Item item;  // 16-byte aligned: filled with uint4 copies
   unsigned long long queue[kQueue];
   unsigned long long unit;
   int qn;
@@ -117,6 +119,9 @@ struct Smem {
   int skip;
   char post[kThreads / 32][kMaxSize + 8];
 };
+
+static_assert(offsetof(Smem, item) % 16 == 0, "Smem::item must be 16-byte aligned");
+static_assert(alignof(Item) == 16, "Item must be 16-byte aligned");
 
 // ------------------------------------------------------------------ device ops
 
@@ -593,7 +598,7 @@ __global__ void build_binary_kernel(W* out, const W* A, const W* B, unsigned lon
   }
 }
 
-__global__ void stamp_start_kernel(unsigned long long* t) { *t = globaltimer_ns(); }
+static __global__ void stamp_start_kernel(unsigned long long* t) { *t = globaltimer_ns(); }
 
 // ------------------------------------------------------------------ host side
 
@@ -723,7 +728,7 @@ struct Enumerator {
 // Structural inversion depth: levels are inverted top-down until the first
 // arithmetic level that lies below an & or | (its constraint mask is then
 // not of the form 2^n - 1).
-static void finish_item(Item& it, int threads, uint64_t mask) {
+static inline void finish_item(Item& it, int threads, uint64_t mask) {
   int inv = it.depth;
   bool andor = false, full = true;
   for (int l = 0; l < it.depth; ++l) {
@@ -1122,27 +1127,13 @@ class Search final : public SearchSession {
   int Tcap_ = 0, built_ = 0, last_T_ = 0;
 };
 
-int make_search_session(const HostInstance& h, const EngineOptions& o, SearchSession** out) {
-  *out = nullptr;
-  int rc = validate(h, 1);
+// Creates and initialises a session for word type W (search_u32.cu / search_u64.cu).
+template <class W>
+int make_search_typed(const HostInstance& h, const EngineOptions& o, SearchSession** out) {
+  auto s = std::make_unique<Search<W>>(h, o);
+  const int rc = s->init();
   if (rc) return rc;
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= o.device || o.device < 0) {
-    cudaGetLastError();
-    set_last_error("no usable CUDA device");
-    return SIMBA_E_NODEV;
-  }
-  if (h.bits == 64) {
-    auto s = std::make_unique<Search<uint64_t>>(h, o);
-    rc = s->init();
-    if (rc) return rc;
-    *out = s.release();
-  } else {
-    auto s = std::make_unique<Search<uint32_t>>(h, o);
-    rc = s->init();
-    if (rc) return rc;
-    *out = s.release();
-  }
+  *out = s.release();
   return 0;
 }
 

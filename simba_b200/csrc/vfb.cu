@@ -1,0 +1,463 @@
+// VFB on sm_100a: bottom-up enumeration of characteristic vectors with
+// observational-equivalence dedup (vfb/src/full-cache.cu:568-774).
+//
+// Same search as the reference: sizes 2..max_len, operators in the order
+// ~ & | ^ neg + - *, unary operators over the rows of size L-1, binary ones
+// over rows(i) x rows(L-1-i) for 2i <= L-1 (Minus also tries the swapped
+// pair), and stop after the operator block that produces the target.
+//
+// Built differently:
+//  * One kernel per (size, operator, split) block; a candidate's vector is
+//    computed element by element from the two operand rows and folded into a
+//    64-bit fingerprint A plus a 32-bit check B on the fly -- never stored.
+//  * Open-addressing hash table (linear probing, power-of-two capacity,
+//    64-bit keys, CAS insert).  A key hit whose published check B differs is
+//    a fingerprint collision and probing continues, so two different vectors
+//    are merged only if both A and B collide.
+//  * A new vector is recomputed, appended with an atomic row counter (no
+//    separate compaction pass) and compared with the target.
+//  * Kernels of a size run back to back on one stream; each one exits at
+//    once if an earlier kernel already found the target, so the host
+//    synchronises once per size instead of after every chunk.
+// reference_dedup = 1 keeps the reference's uniqueness test as written: a
+// vector is stored when the hash set already held it and dropped on a fresh
+// insert (warpcore HashSet::insert returns i+1 > 0 for a present key,
+// vfb/include/warpcore/hash_set.cuh:210-214,230-233, and the caller keeps
+// `insert(...) > 0`, full-cache.cu:285-286).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "cuda_util.h"
+#include "engine.h"
+#include "grammar.h"
+
+namespace simba {
+
+constexpr unsigned long long kEmptyKey = ~0ULL;
+
+template <class W>
+struct VfbArgs {
+  W* rows;                    // [cap][S] row-major characteristic vectors
+  int8_t* rop;                // provenance: operator (-1 = variable)
+  uint32_t* rl;               //             left operand row
+  uint32_t* rr;               //             right operand row
+  unsigned long long* keys;   // hash keys (fingerprint A), kEmptyKey = free
+  unsigned* vals;             // hash check B (0 = not yet published)
+  unsigned long long mask;    // hash capacity - 1
+  unsigned long long* nrows;  // row counter
+  unsigned long long cap;     // row capacity
+  const W* target;            // S words
+  unsigned long long* found;  // (left << 32) | right of the matching candidate
+  int* found_launch;          // launch id that found the target (INT_MAX = none)
+  int* flags;                 // [0] cache full, [1] hash full
+  unsigned long long l0, nl, r0, nr;
+  int S;
+  int swap;                   // Minus: also op(right, left)
+  int inverted;               // reference dedup semantics
+  int launch;                 // id of this launch within the search
+};
+
+template <class W, int OP>
+__device__ __forceinline__ W vop(W l, W r) {
+  if (OP == OP_NOT) return (W)~l;
+  if (OP == OP_NEG) return (W)(W(0) - l);
+  if (OP == OP_AND) return l & r;
+  if (OP == OP_OR) return l | r;
+  if (OP == OP_XOR) return l ^ r;
+  if (OP == OP_ADD) return (W)(l + r);
+  if (OP == OP_SUB) return (W)(l - r);
+  return (W)(l * r);
+}
+
+// Fingerprint: A is a multiply-xorshift fold finished with the MurmurHash3
+// 64-bit finaliser (Appleby); B is an independent position-weighted sum.
+__device__ __forceinline__ void fp_step(unsigned long long& a, unsigned long long& b,
+                                        unsigned long long x, int i) {
+  a ^= x;
+  a *= 0x9E3779B97F4A7C15ULL;
+  a ^= a >> 29;
+  b += x * (0xD6E8FEB86659FD93ULL + 2ULL * (unsigned long long)i);
+}
+
+__device__ __forceinline__ unsigned long long fp_final(unsigned long long a, int S) {
+  a ^= (unsigned long long)S;
+  a ^= a >> 33;
+  a *= 0xff51afd7ed558ccdULL;
+  a ^= a >> 33;
+  a *= 0xc4ceb9fe1a85ec53ULL;
+  a ^= a >> 33;
+  return a == kEmptyKey ? kEmptyKey - 1 : a;
+}
+
+__device__ __forceinline__ unsigned fp_check(unsigned long long b) {
+  unsigned c = (unsigned)(b ^ (b >> 32));
+  return c ? c : 1u;
+}
+
+enum { INS_NEW = 0, INS_DUP = 1, INS_FULL = 2 };
+
+__device__ int hash_insert(unsigned long long* keys, unsigned* vals, unsigned long long mask,
+                           unsigned long long A, unsigned B) {
+  for (unsigned long long p = 0; p <= mask; ++p) {
+    const unsigned long long s = (A + p) & mask;
+    unsigned long long k = keys[s];
+    if (k == kEmptyKey) {
+      const unsigned long long old = atomicCAS(&keys[s], kEmptyKey, A);
+      if (old == kEmptyKey) {
+        atomicExch(&vals[s], B);
+        return INS_NEW;
+      }
+      k = old;
+    }
+    if (k == A) {
+      const unsigned v = *(volatile unsigned*)&vals[s];
+      if (v == 0 || v == B) return INS_DUP;  // unpublished: same key, treat as equal
+    }
+  }
+  return INS_FULL;
+}
+
+template <class W, int OP>
+__global__ void __launch_bounds__(256) vfb_compose_kernel(VfbArgs<W> a) {
+  if (*(volatile int*)a.found_launch < a.launch) return;  // an earlier block found it
+  constexpr bool unary = OP == OP_NOT || OP == OP_NEG;
+  const unsigned long long per = unary ? a.nl : a.nl * a.nr;
+  const unsigned long long total = per << (a.swap ? 1 : 0);
+  const int S = a.S;
+  for (unsigned long long idx = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long pair = a.swap ? idx >> 1 : idx;
+    unsigned long long x, y;
+    if (unary) {
+      x = a.l0 + pair;
+      y = 0;
+    } else {
+      const unsigned long long li = pair / a.nr;
+      x = a.l0 + li;
+      y = a.r0 + (pair - li * a.nr);
+      if (a.swap && (idx & 1)) {
+        const unsigned long long t = x;
+        x = y;
+        y = t;
+      }
+    }
+    const W* L = a.rows + x * S;
+    const W* R = a.rows + y * S;
+    unsigned long long fa = 0x243F6A8885A308D3ULL, fb = 0;
+    for (int i = 0; i < S; ++i) {
+      const W v = vop<W, OP>(L[i], unary ? W(0) : R[i]);
+      fp_step(fa, fb, (unsigned long long)v, i);
+    }
+    const unsigned long long A = fp_final(fa, S);
+    const unsigned B = fp_check(fb);
+    const int ins = hash_insert(a.keys, a.vals, a.mask, A, B);
+    bool keep;
+    if (a.inverted) keep = ins != INS_NEW;  // INS_FULL is kept too, as in the reference
+    else {
+      if (ins == INS_FULL) atomicOr(&a.flags[1], 1);
+      keep = ins == INS_NEW;
+    }
+    if (!keep) continue;
+    const unsigned long long row = atomicAdd(a.nrows, 1ULL);
+    bool match = true;
+    W* out = row < a.cap ? a.rows + row * S : nullptr;
+    for (int i = 0; i < S; ++i) {
+      const W v = vop<W, OP>(L[i], unary ? W(0) : R[i]);
+      match &= v == a.target[i];
+      if (out) out[i] = v;
+    }
+    if (out) {
+      a.rop[row] = (int8_t)OP;
+      a.rl[row] = (uint32_t)x;
+      a.rr[row] = (uint32_t)y;
+    } else {
+      atomicOr(&a.flags[0], 1);
+    }
+    if (match) {
+      atomicCAS(a.found, ~0ULL, (x << 32) | y);
+      atomicMin(a.found_launch, a.launch);
+    }
+  }
+}
+
+template <class W>
+__global__ void vfb_init_kernel(VfbArgs<W> a, int k) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= k) return;
+  const W* v = a.rows + (unsigned long long)j * a.S;
+  unsigned long long fa = 0x243F6A8885A308D3ULL, fb = 0;
+  for (int i = 0; i < a.S; ++i) fp_step(fa, fb, (unsigned long long)v[i], i);
+  hash_insert(a.keys, a.vals, a.mask, fp_final(fa, a.S), fp_check(fb));
+  a.rop[j] = -1;
+  a.rl[j] = (uint32_t)j;
+  a.rr[j] = 0;
+}
+
+template <class W>
+static void launch_compose(int op, int grid, cudaStream_t st, const VfbArgs<W>& a) {
+  switch (op) {
+    case OP_NOT: vfb_compose_kernel<W, OP_NOT><<<grid, 256, 0, st>>>(a); break;
+    case OP_AND: vfb_compose_kernel<W, OP_AND><<<grid, 256, 0, st>>>(a); break;
+    case OP_OR: vfb_compose_kernel<W, OP_OR><<<grid, 256, 0, st>>>(a); break;
+    case OP_XOR: vfb_compose_kernel<W, OP_XOR><<<grid, 256, 0, st>>>(a); break;
+    case OP_NEG: vfb_compose_kernel<W, OP_NEG><<<grid, 256, 0, st>>>(a); break;
+    case OP_ADD: vfb_compose_kernel<W, OP_ADD><<<grid, 256, 0, st>>>(a); break;
+    case OP_SUB: vfb_compose_kernel<W, OP_SUB><<<grid, 256, 0, st>>>(a); break;
+    default: vfb_compose_kernel<W, OP_MUL><<<grid, 256, 0, st>>>(a); break;
+  }
+}
+
+template <class W>
+static int vfb_typed(const HostInstance& h, int max_len, const EngineOptions& o, int inverted,
+                     int64_t cache_rows, VfbOutcome* out) {
+  *out = VfbOutcome();
+  const int S = h.S, k = h.k;
+  SB_CUDA(cudaSetDevice(o.device));
+  cudaStream_t st = nullptr;
+  bool own = false;
+  if (o.stream) st = reinterpret_cast<cudaStream_t>(o.stream);
+  else {
+    SB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    own = true;
+  }
+  struct StreamGuard {
+    cudaStream_t s;
+    bool own;
+    ~StreamGuard() {
+      if (own && s) cudaStreamDestroy(s);
+    }
+  } guard{st, own};
+  int sms = 0;
+  SB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, o.device));
+  // Row capacity: the reference's rule (max pitch / (S * 4 bytes),
+  // full-cache.cu:713-718) unless the caller sets one.
+  unsigned long long cap = (unsigned long long)cache_rows;
+  if (cap == 0) {
+    int pitch = 0;
+    SB_CUDA(cudaDeviceGetAttribute(&pitch, cudaDevAttrMaxPitch, o.device));
+    cap = (unsigned long long)pitch / ((unsigned long long)S * 4ULL);
+  }
+  cap = std::max<unsigned long long>(cap, (unsigned long long)k + 1);
+  cap = std::min<unsigned long long>(cap, 0xFFFFFFF0ULL);
+  unsigned long long slots = 1;
+  while (slots < cap * (inverted ? 4 : 2)) slots <<= 1;
+  DevBuf rows, rop, rl, rr, keys, vals, scal, tgt;
+  SB_CUDA(rows.reserve(cap * S * sizeof(W)));
+  SB_CUDA(rop.reserve(cap));
+  SB_CUDA(rl.reserve(cap * 4));
+  SB_CUDA(rr.reserve(cap * 4));
+  SB_CUDA(keys.reserve(slots * 8));
+  SB_CUDA(vals.reserve(slots * 4));
+  SB_CUDA(scal.reserve(64));
+  SB_CUDA(tgt.reserve(S * sizeof(W)));
+  out->cache_bytes = cap * S * sizeof(W) + cap * 9;
+  out->table_bytes = slots * 12;
+  SB_CUDA(cudaMemsetAsync(keys.p, 0xFF, slots * 8, st));
+  SB_CUDA(cudaMemsetAsync(vals.p, 0, slots * 4, st));
+  // scalars: [0] nrows, [1] found pair, [2] found_launch|flags
+  unsigned long long init[4] = {(unsigned long long)k, ~0ULL, 0, 0};
+  SB_CUDA(cudaMemcpyAsync(scal.p, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  int* iflags = reinterpret_cast<int*>(scal.as<unsigned long long>() + 2);
+  const int fl_init[4] = {INT_MAX, 0, 0, 0};
+  SB_CUDA(cudaMemcpyAsync(iflags, fl_init, sizeof(fl_init), cudaMemcpyHostToDevice, st));
+  std::vector<W> hv((size_t)k * S), ht(S);
+  for (int j = 0; j < k; ++j)
+    for (int i = 0; i < S; ++i) hv[(size_t)j * S + i] = (W)h.in[(size_t)i * k + j];
+  for (int i = 0; i < S; ++i) ht[i] = (W)h.out[i];
+  SB_CUDA(cudaMemcpyAsync(rows.p, hv.data(), hv.size() * sizeof(W), cudaMemcpyHostToDevice, st));
+  SB_CUDA(cudaMemcpyAsync(tgt.p, ht.data(), ht.size() * sizeof(W), cudaMemcpyHostToDevice, st));
+
+  VfbArgs<W> a;
+  memset(&a, 0, sizeof(a));
+  a.rows = rows.as<W>();
+  a.rop = rop.as<int8_t>();
+  a.rl = rl.as<uint32_t>();
+  a.rr = rr.as<uint32_t>();
+  a.keys = keys.as<unsigned long long>();
+  a.vals = vals.as<unsigned>();
+  a.mask = slots - 1;
+  a.nrows = scal.as<unsigned long long>();
+  a.cap = cap;
+  a.target = tgt.as<W>();
+  a.found = scal.as<unsigned long long>() + 1;
+  a.found_launch = iflags;
+  a.flags = iflags + 1;
+  a.S = S;
+  a.inverted = inverted;
+
+  const auto t0 = std::chrono::steady_clock::now();
+  // size 1: the variables (full-cache.cu:694-707), checked on the host
+  for (int j = 0; j < k; ++j) {
+    out->candidates++;
+    bool eq = true;
+    for (int i = 0; i < S && eq; ++i) eq = (W)h.in[(size_t)i * k + j] == (W)h.out[i];
+    if (eq) {
+      out->status = SIMBA_OK;
+      out->size = 1;
+      out->op = 8;
+      out->postfix = std::string(1, (char)('0' + j));
+      out->rows_per_size[1] = k;
+      out->rows_total = k;
+      return SIMBA_OK;
+    }
+  }
+  cudaEvent_t e0, e1;
+  SB_CUDA(cudaEventCreate(&e0));
+  SB_CUDA(cudaEventCreate(&e1));
+  SB_CUDA(cudaEventRecord(e0, st));
+  vfb_init_kernel<W><<<(k + 63) / 64, 64, 0, st>>>(a, k);
+  out->launches++;
+  SB_CUDA(cudaGetLastError());
+  std::vector<unsigned long long> start(max_len + 3, 0);
+  start[1] = 0;
+  start[2] = (unsigned long long)k;
+  out->rows_per_size[1] = k;
+  const int grid = sms * 8;
+  int launch = 0;
+  struct LaunchInfo {
+    int op;
+    unsigned long long cand;
+  };
+  std::vector<LaunchInfo> info;
+  unsigned long long hs[4];
+  int status = SIMBA_NOT_FOUND;
+  for (int L = 2; L <= max_len; ++L) {
+    if (o.budget_s > 0 &&
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > o.budget_s) {
+      status = SIMBA_BUDGET;
+      break;
+    }
+    info.clear();
+    const int first_launch = launch;
+    for (int op = 0; op < 8; ++op) {
+      if (is_unary(op)) {
+        a.l0 = start[L - 1];
+        a.nl = start[L] - start[L - 1];
+        a.r0 = 0;
+        a.nr = 1;
+        a.swap = 0;
+        if (a.nl == 0) continue;
+        a.launch = launch++;
+        info.push_back({op, a.nl});
+        launch_compose<W>(op, (int)std::min<unsigned long long>((a.nl + 255) / 256, grid), st, a);
+      } else {
+        for (int i = 1; 2 * i <= L - 1; ++i) {
+          const int j = L - 1 - i;
+          a.l0 = start[i];
+          a.nl = start[i + 1] - start[i];
+          a.r0 = start[j];
+          a.nr = start[j + 1] - start[j];
+          a.swap = op == OP_SUB ? 1 : 0;
+          const unsigned long long n = (a.nl * a.nr) << a.swap;
+          if (n == 0) continue;
+          a.launch = launch++;
+          info.push_back({op, n});
+          launch_compose<W>(op, (int)std::min<unsigned long long>((n + 255) / 256, grid), st, a);
+        }
+      }
+    }
+    SB_CUDA(cudaGetLastError());
+    out->launches = launch + 1;
+    SB_CUDA(cudaMemcpyAsync(hs, scal.p, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    SB_CUDA(cudaStreamSynchronize(st));
+    const int fl = (int)(hs[2] & 0xFFFFFFFFULL);
+    const int full = (int)(hs[2] >> 32);
+    const int hfull = (int)(hs[3] & 0xFFFFFFFFULL);
+    const unsigned long long nrows = std::min<unsigned long long>(hs[0], cap);
+    // reference-rule candidate count: every launch up to the one that found
+    for (size_t q = 0; q < info.size(); ++q)
+      if (fl == INT_MAX || first_launch + (int)q <= fl) out->candidates += info[q].cand;
+    start[L + 1] = nrows;
+    out->rows_per_size[L] = (int64_t)(nrows - start[L]);
+    out->rows_total = (int64_t)nrows;
+    out->max_size_searched = L;
+    if (o.verbose)
+      fprintf(stderr, "vfb size %2d | rows %llu | candidates %llu\n", L, nrows,
+              (unsigned long long)out->candidates);
+    if (fl != INT_MAX) {
+      out->status = SIMBA_OK;
+      out->size = L;
+      out->op = info[fl - first_launch].op;
+      // reconstruct the expression from the provenance arrays
+      const unsigned long long pair = hs[1];
+      std::string post;
+      struct Node {
+        static int build(const DevBuf& rop, const DevBuf& rl, const DevBuf& rr, unsigned long long row,
+                         int k, std::string* p, int depth) {
+          if (depth > 200) return -1;
+          if (row < (unsigned long long)k) {
+            p->push_back((char)('0' + (int)row));
+            return 0;
+          }
+          int8_t op;
+          uint32_t l, r;
+          if (cudaMemcpy(&op, rop.as<int8_t>() + row, 1, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+          if (cudaMemcpy(&l, rl.as<uint32_t>() + row, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+          if (cudaMemcpy(&r, rr.as<uint32_t>() + row, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+          if (build(rop, rl, rr, l, k, p, depth + 1)) return -1;
+          if (!is_unary(op) && build(rop, rl, rr, r, k, p, depth + 1)) return -1;
+          p->push_back(op_char(op));
+          return 0;
+        }
+      };
+      const unsigned long long x = pair >> 32, y = pair & 0xFFFFFFFFULL;
+      int rc = Node::build(rop, rl, rr, x, k, &post, 0);
+      if (!rc && !is_unary(out->op)) rc = Node::build(rop, rl, rr, y, k, &post, 0);
+      if (rc) {
+        set_last_error("VFB expression reconstruction failed");
+        return SIMBA_E_INTERNAL;
+      }
+      post.push_back(op_char(out->op));
+      out->postfix = post;
+      status = SIMBA_OK;
+      break;
+    }
+    if (full || hfull) {
+      status = SIMBA_CACHE_FULL;
+      break;
+    }
+  }
+  SB_CUDA(cudaEventRecord(e1, st));
+  SB_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  out->device_ms = ms;
+  out->status = status;
+  // algorithmic bytes: two operand rows per candidate (one for unary), one
+  // 12-byte hash probe, one written row per stored vector
+  out->bytes_moved = (double)out->candidates * (2.0 * S * sizeof(W) + 12.0) +
+                     (double)out->rows_total * S * sizeof(W);
+  if (status == SIMBA_OK && !host_check(out->postfix, h)) {
+    set_last_error("VFB answer failed the host re-check");
+    return SIMBA_E_INTERNAL;
+  }
+  return status;
+}
+
+int vfb_run(const HostInstance& h, int max_len, const EngineOptions& o, int inverted, int64_t cache_rows,
+            VfbOutcome* out) {
+  int rc = validate(h, 1);
+  if (rc) return rc;
+  if (max_len < 1 || max_len > 100) {
+    set_last_error("maxLen must be between 1 and 100");
+    return SIMBA_E_ARG;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= o.device || o.device < 0) {
+    cudaGetLastError();
+    set_last_error("no usable CUDA device");
+    return SIMBA_E_NODEV;
+  }
+  if (h.bits == 64) return vfb_typed<uint64_t>(h, max_len, o, inverted, cache_rows, out);
+  return vfb_typed<uint32_t>(h, max_len, o, inverted, cache_rows, out);
+}
+
+}  // namespace simba
