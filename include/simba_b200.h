@@ -118,6 +118,20 @@ typedef struct {
 int vfb_solve(const simba_instance *inst, int max_len, const simba_options *opt,
               vfb_result *result);
 
+/* simba_solve without any device allocation, for callers that cannot call
+ * cudaMalloc while they run (a plugin inside a host application that owns
+ * the GPU memory budget, or code running while another stream is being
+ * captured into a CUDA graph).  No counterpart in the reference.  All
+ * scratch lives in one 64 MiB __device__ array that every GPU loading the
+ * library holds until exit; sizes whose value tables or spine list do not
+ * fit it are rejected with SIMBA_E_ARG.  The first call on a device looks up
+ * that array's address, so make it before any stream capture starts.  Calls
+ * share the array: calls that overlap on the GPU race and must be
+ * serialised.  Runs on opt->stream (0 = default stream); creates no stream
+ * or event and reports only host-clock seconds. */
+int simba_solve_noalloc(const simba_instance *inst, int max_size, const simba_options *opt,
+                        simba_result *result);
+
 /* Resident session: samples and value tables stay on the device between
  * calls (used by the benchmark to time the search with inputs in HBM). */
 typedef struct simba_session simba_session;

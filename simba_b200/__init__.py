@@ -96,6 +96,7 @@ def lib():
     L.simba_device_count.restype = C.c_int
     L.simba_int_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
     L.vfb_solve.argtypes = [P(_Instance), C.c_int, P(_Options), P(_VfbResult)]
+    L.simba_solve_noalloc.argtypes = [P(_Instance), C.c_int, P(_Options), P(_Result)]
     _lib = L
     return L
 
@@ -167,6 +168,17 @@ def solve(inst: Instance, max_size: int, **kw) -> Result:
     a = _Arrays(inst)
     r = _Result()
     rc = lib().simba_solve(C.byref(a.c), max_size, C.byref(_opts(**kw)), C.byref(r))
+    _check(rc)
+    return _res(r)
+
+
+def solve_noalloc(inst: Instance, max_size: int, **kw) -> Result:
+    """Same search as :func:`solve` with every scratch buffer in the library's
+    static 64 MiB device array: for callers that cannot allocate device
+    memory while they run.  Calls share that array; do not overlap them."""
+    a = _Arrays(inst)
+    r = _Result()
+    rc = lib().simba_solve_noalloc(C.byref(a.c), max_size, C.byref(_opts(**kw)), C.byref(r))
     _check(rc)
     return _res(r)
 

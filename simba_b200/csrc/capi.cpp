@@ -275,6 +275,29 @@ int simba_solve(const simba_instance* inst, int max_size, const simba_options* o
   return result->status;
 }
 
+int simba_solve_noalloc(const simba_instance* inst, int max_size, const simba_options* opt,
+                        simba_result* result) {
+  if (!result) return SIMBA_E_ARG;
+  memset(result, 0, sizeof(*result));
+  const auto t0 = std::chrono::steady_clock::now();
+  HostInstance h;
+  int rc = to_host(inst, &h);
+  if (!rc) rc = validate(h, max_size);
+  if (rc) {
+    result->status = rc;
+    return rc;
+  }
+  SolveOutcome oc;
+  rc = solve_static(h, max_size, to_opts(opt), &oc);
+  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (rc < 0) {
+    result->status = rc;
+    return rc;
+  }
+  fill_result(oc, secs, result);
+  return result->status;
+}
+
 int simba_session_create(const simba_instance* inst, const simba_options* opt,
                          simba_session** session) {
   if (!session) return SIMBA_E_ARG;

@@ -69,6 +69,9 @@ class SearchSession {
 int make_search_session(const HostInstance& h, const EngineOptions& o,
                         SearchSession** out);
 
+// Plain search with all scratch in a static __device__ array (search_static.cu).
+int solve_static(const HostInstance& h, int max_size, const EngineOptions& o, SolveOutcome* out);
+
 // Read an instance file in the reference JSON schema.
 int read_instance_json(const std::string& path, HostInstance* h);
 

@@ -1,0 +1,50 @@
+"""simba_solve_noalloc: the allocation-free entry point, checked against
+simba_solve through the C ABI.
+
+It serves callers that cannot allocate device memory while they run, so all
+of its scratch lives in the library's static device array; this file is
+collected last so that a failure here leaves every other test already run.
+Two calls in a row must agree with the allocating entry point (the array
+keeps the previous call's contents, which the search must not depend on).
+"""
+import pytest
+
+import simba_b200 as S
+from simba_b200.instances import Instance, make_instance
+
+pytestmark = pytest.mark.gpu
+
+
+def key(r):
+    return (r.status, r.size, r.op, r.rank, r.postfix, r.candidates, tuple(r.per_size))
+
+
+def cases(golden):
+    out = [Instance.from_json(golden["instances"][i]) for i in (0, 40, 80, 113)]
+    out += [make_instance(9, 2, 32, 0, word_bits=64),
+            make_instance(11, 3, 64, 21, word_bits=64),
+            make_instance(10, 2, 16, 5, word_bits=32)]
+    return out
+
+
+def test_noalloc_matches_simba_solve_twice_in_a_row(golden):
+    for inst in cases(golden):
+        ref = S.solve(inst, 13)
+        first = S.solve_noalloc(inst, 13)
+        second = S.solve_noalloc(inst, 13)
+        assert key(first) == key(ref)
+        assert key(second) == key(ref)
+
+
+def test_noalloc_unsat_sweep_matches(golden):
+    inst = make_instance(12, 3, 64, 9, word_bits=64, unsat=True)
+    ref = S.solve(inst, 12)
+    for _ in range(2):
+        r = S.solve_noalloc(inst, 12)
+        assert key(r) == key(ref) and r.status == S.NOT_FOUND
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch():
+    inst = make_instance(15, 3, 64, 9, word_bits=64, unsat=True)
+    with pytest.raises(S.SimbaError, match="static scratch"):
+        S.solve_noalloc(inst, 20)
