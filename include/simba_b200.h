@@ -142,6 +142,23 @@ int simba_session_solve(simba_session *session, int max_size, simba_result *resu
 int simba_session_sweep(simba_session *session, int lo, int hi, simba_result *result);
 void simba_session_destroy(simba_session *session);
 
+/* One size of the plain search over the work units u with
+ * u % nshards == shard: the building block of a search spread over several
+ * GPUs, where each GPU takes one shard and the minimum of the shards'
+ * best_rank decides the size (no counterpart in the reference, which uses
+ * one GPU). */
+typedef struct {
+  int32_t status;        /* SIMBA_OK if this shard holds a match                 */
+  int32_t launches;
+  uint64_t best_rank;    /* minimum matching rank in this shard, ~0 if none      */
+  uint64_t candidates;   /* candidates of the whole size                         */
+  uint64_t evaluated;    /* candidates this shard evaluated                      */
+  double device_ms;
+  double kernel_ms;
+} simba_size_result;
+int simba_session_search_size(simba_session *session, int size, int shard, int nshards,
+                              simba_size_result *result);
+
 /* Count table numForm[size][op] (simba/src/nocache.cu:117-160), written as
  * (max_size + 1) rows of 9 columns, column 8 = total.  Host only. */
 int simba_count_table(int max_size, int n_terms, uint64_t *table);

@@ -46,6 +46,12 @@ class _Options(C.Structure):
                 ("reserved", C.c_int32 * 3)]
 
 
+class _SizeResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("launches", C.c_int32), ("best_rank", C.c_uint64),
+                ("candidates", C.c_uint64), ("evaluated", C.c_uint64),
+                ("device_ms", C.c_double), ("kernel_ms", C.c_double)]
+
+
 class _VfbResult(C.Structure):
     _fields_ = [("status", C.c_int32), ("size", C.c_int32), ("op", C.c_int32),
                 ("max_size_searched", C.c_int32), ("postfix", C.c_char * 256),
@@ -97,6 +103,8 @@ def lib():
     L.simba_int_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
     L.vfb_solve.argtypes = [P(_Instance), C.c_int, P(_Options), P(_VfbResult)]
     L.simba_solve_noalloc.argtypes = [P(_Instance), C.c_int, P(_Options), P(_Result)]
+    L.simba_session_search_size.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                            P(_SizeResult)]
     _lib = L
     return L
 
@@ -236,6 +244,15 @@ class Session:
         r = _Result()
         _check(lib().simba_session_sweep(self._h, lo, hi, C.byref(r)))
         return _res(r)
+
+    def search_size(self, size: int, shard: int = 0, nshards: int = 1) -> dict:
+        """One size over work units u % nshards == shard; best_rank is the
+        minimum matching rank in this shard (None if none)."""
+        r = _SizeResult()
+        _check(lib().simba_session_search_size(self._h, size, shard, nshards, C.byref(r)))
+        return {"status": r.status, "best_rank": None if r.best_rank == 2 ** 64 - 1 else
+                r.best_rank, "candidates": r.candidates, "evaluated": r.evaluated,
+                "device_ms": r.device_ms, "kernel_ms": r.kernel_ms, "launches": r.launches}
 
     def close(self) -> None:
         if self._h:

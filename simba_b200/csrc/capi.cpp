@@ -386,6 +386,26 @@ int vfb_solve(const simba_instance* inst, int max_len, const simba_options* opt,
   return result->status;
 }
 
+int simba_session_search_size(simba_session* session, int size, int shard, int nshards,
+                              simba_size_result* result) {
+  if (!session || !result) return SIMBA_E_ARG;
+  memset(result, 0, sizeof(*result));
+  SizeOutcome oc;
+  const int rc = session->s->search_one_size(size, shard, nshards, &oc);
+  if (rc < 0) {
+    result->status = rc;
+    return rc;
+  }
+  result->status = oc.status;
+  result->launches = oc.launches;
+  result->best_rank = oc.best;
+  result->candidates = oc.candidates;
+  result->evaluated = oc.evaluated;
+  result->device_ms = oc.device_ms;
+  result->kernel_ms = oc.kernel_ms;
+  return oc.status;
+}
+
 void simba_session_destroy(simba_session* session) {
   if (!session) return;
   delete session->s;

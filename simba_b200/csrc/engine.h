@@ -58,9 +58,20 @@ int validate(const HostInstance& h, int max_size);
 
 // Plain SIMBA search on one instance.  Session objects keep the samples and
 // value tables resident between calls.
+struct SizeOutcome {
+  int status = SIMBA_NOT_FOUND;
+  uint64_t best = ~0ULL;
+  uint64_t candidates = 0;
+  uint64_t evaluated = 0;
+  double device_ms = 0.0;
+  double kernel_ms = 0.0;
+  int launches = 0;
+};
+
 class SearchSession {
  public:
   virtual ~SearchSession() = default;
+  virtual int search_one_size(int size, int shard, int nshards, SizeOutcome* out) = 0;
   virtual int solve(int max_size, SolveOutcome* out) = 0;
   // Evaluate every candidate of sizes [lo, hi] with no early stop.
   virtual int sweep(int lo, int hi, SolveOutcome* out) = 0;

@@ -55,7 +55,7 @@ constexpr int kMaxDepth = 12;  // spine levels
 constexpr int kThreads = 256;  // CTA size of the search kernels
 constexpr int kQueue = 128;    // shared-memory queue of sample-0 matches
 constexpr int kR = 4;          // contexts per thread
-constexpr int kMaxExplicit = 4;
+constexpr int kMaxExplicit = 2;
 
 // One level of a spine, top-down (level 0 is the root).
 struct Level {
@@ -82,8 +82,19 @@ struct alignas(16) Item {
   uint32_t cb;          // contexts per unit = G * kR
   uint16_t G, L;        // G context groups x L value lanes = kThreads
   int8_t depth, inv, bottom, full, nexp;
-  int8_t pad[19];
+  int8_t fused;         // 1: contexts are read from the materialised list
+  int8_t pad[2];
+  uint64_t ctx_off;     // fused: first context in Params::ctxs
+  uint64_t pad2;
   Level lv[kMaxDepth];
+};
+
+// A materialised context of a fused group: the bottom-value constraint
+// (v & M) == K and the rank of candidate v = base + v * coefv.
+template <class W>
+struct Ctx {
+  W M, K;
+  unsigned long long base, coefv;
 };
 static_assert(sizeof(Item) % 16 == 0, "Item must be 16-byte sized");
 
@@ -91,6 +102,10 @@ template <class W>
 struct Params {
   const W* tab[kMaxSize + 1];
   const Item* items;
+  const Ctx<W>* ctxs;     // materialised contexts of fused groups
+  const Item* sitems;     // spines whose contexts are materialised
+  int nsitems;
+  unsigned long long nctxs;
   const W* in;
   const W* out;
   const unsigned long long* counts;
@@ -100,6 +115,8 @@ struct Params {
   unsigned long long* start_ns;
   int* flags;  // [0] budget expired, [1] inversion failure, [2] queue overflows
   unsigned long long total_units;
+  unsigned long long unit_offset;  // this shard's first unit (multi-GPU)
+  unsigned long long unit_stride;  // number of shards (0 is read as 1)
   unsigned long long budget_ns;
   W target;
   int nitems;
@@ -335,8 +352,9 @@ __device__ __forceinline__ W eval_explicit(const Explicit<W>& X, const W* w, W x
 }
 
 // One work unit: kR contexts per thread x a strided share of the bottom
-// values.  Loads are 16-byte vectors of the bottom table.
-template <class W, int E, bool FULL>
+// values.  Loads are 16-byte vectors of the bottom table, four in flight per
+// thread.  FUSED units take their contexts from the materialised list.
+template <class W, int E, bool FULL, bool FUSED>
 __device__ void process_unit(const Params<W>& p, Smem& sm, const Item& it, unsigned long long local,
                              const W* s_in, const W* s_out) {
   constexpr int VW = 16 / sizeof(W);
@@ -365,6 +383,12 @@ __device__ void process_unit(const Params<W>& p, Smem& sm, const Item& it, unsig
   for (int r = 0; r < kR; ++r) {
     const unsigned long long c = c0 + r < it.nctx ? c0 + r : c0;  // pad with a duplicate
     if (c0 + r < it.nctx) valid |= 1u << r;
+    if (FUSED) {
+      const Ctx<W> cx = p.ctxs[it.ctx_off + (c < it.nctx ? c : 0)];
+      M[r] = cx.M;
+      K[r] = cx.K;
+      continue;
+    }
     W wl[kMaxDepth];
     decode_context<W>(p, it, c, wl);
     W m = (W)~W(0), k = p.target;
@@ -384,8 +408,7 @@ __device__ void process_unit(const Params<W>& p, Smem& sm, const Item& it, unsig
   const unsigned long long q0 = v0 / VW, q1 = (v1 + VW - 1) / VW;
   const uint4* V4 = reinterpret_cast<const uint4*>(V);
 
-  for (unsigned long long q = q0 + lane; q < q1; q += L) {
-    const uint4 raw = __ldg(V4 + q);
+  auto test = [&](const uint4& raw, unsigned long long q) {
     W xs[VW];
     memcpy(xs, &raw, 16);
     bool hit = false;
@@ -398,23 +421,69 @@ __device__ void process_unit(const Params<W>& p, Smem& sm, const Item& it, unsig
         hit |= FULL ? (y == K[r]) : ((W)(y & M[r]) == K[r]);
       }
     }
-    if (hit) {
-#pragma unroll
-      for (int e = 0; e < VW; ++e) {
-        const unsigned long long v = q * VW + e;
-        if (v < v0 || v >= v1) continue;
-        for (int r = 0; r < kR; ++r) {
-          if (!(valid >> r & 1)) continue;
-          W y = xs[e];
-          if (E > 0) y = eval_explicit<W, E>(X, WX[r], y);
-          const bool h = FULL ? (y == K[r]) : ((W)(y & M[r]) == K[r]);
-          if (h) {
-            const unsigned long long rank = decode_context<W>(p, it, c0 + r, nullptr) + v * it.coefv;
-            push_hit<W>(p, sm, s_in, s_out, rank);
-          }
+    if (!hit) return;
+    for (int e = 0; e < VW; ++e) {
+      const unsigned long long v = q * VW + e;
+      if (v < v0 || v >= v1) continue;
+      for (int r = 0; r < kR; ++r) {
+        if (!(valid >> r & 1)) continue;
+        W y = xs[e];
+        if (E > 0) y = eval_explicit<W, E>(X, WX[r], y);
+        const bool h = FULL ? (y == K[r]) : ((W)(y & M[r]) == K[r]);
+        if (!h) continue;
+        unsigned long long rank;
+        if (FUSED) {
+          const Ctx<W> cx = p.ctxs[it.ctx_off + c0 + r];
+          rank = cx.base + v * cx.coefv;
+        } else {
+          rank = decode_context<W>(p, it, c0 + r, nullptr) + v * it.coefv;
         }
+        push_hit<W>(p, sm, s_in, s_out, rank);
       }
     }
+  };
+
+  unsigned long long q = q0 + lane;
+  const unsigned long long step = (unsigned long long)L;
+  if (E == 0) {  // four loads in flight; explicit levels keep one (code size)
+    for (; q + 3 * step < q1; q += 4 * step) {
+      const uint4 a0 = __ldg(V4 + q);
+      const uint4 a1 = __ldg(V4 + q + step);
+      const uint4 a2 = __ldg(V4 + q + 2 * step);
+      const uint4 a3 = __ldg(V4 + q + 3 * step);
+      test(a0, q);
+      test(a1, q + step);
+      test(a2, q + 2 * step);
+      test(a3, q + 3 * step);
+    }
+  }
+  for (; q < q1; q += step) test(__ldg(V4 + q), q);
+}
+
+// Materialise the contexts of the spines listed in p.sitems: one thread per
+// context writes its fully inverted constraint and rank coefficients.
+template <class W>
+__global__ void __launch_bounds__(256) materialize_kernel(Params<W> p, Ctx<W>* out) {
+  for (unsigned long long gi = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; gi < p.nctxs;
+       gi += (unsigned long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = p.nsitems - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (p.sitems[mid].ctx_off <= gi) lo = mid;
+      else hi = mid - 1;
+    }
+    const Item& it = p.sitems[lo];
+    const unsigned long long c = gi - it.ctx_off;
+    W wl[kMaxDepth];
+    Ctx<W> cx;
+    cx.base = decode_context<W>(p, it, c, wl);
+    cx.coefv = it.coefv;
+    W m = (W)~W(0), k = p.target;
+    for (int l = 0; l < it.depth; ++l)
+      if (!invert_level<W>(it.lv[l], wl[l], m, k)) atomicOr(&p.flags[1], 1);
+    cx.M = m;
+    cx.K = k;
+    out[gi] = cx;
   }
 }
 
@@ -450,22 +519,22 @@ template <class W>
 __device__ void dispatch_unit(const Params<W>& p, Smem& sm, const Item& it, unsigned long long local,
                               const W* s_in, const W* s_out) {
   const int e = it.nexp;
+  if (it.fused) {
+    if (it.full) return process_unit<W, 0, true, true>(p, sm, it, local, s_in, s_out);
+    return process_unit<W, 0, false, true>(p, sm, it, local, s_in, s_out);
+  }
   if (e > kMaxExplicit) return process_unit_generic<W>(p, sm, it, local, s_in, s_out);
   if (it.full) {
     switch (e) {
-      case 0: return process_unit<W, 0, true>(p, sm, it, local, s_in, s_out);
-      case 1: return process_unit<W, 1, true>(p, sm, it, local, s_in, s_out);
-      case 2: return process_unit<W, 2, true>(p, sm, it, local, s_in, s_out);
-      case 3: return process_unit<W, 3, true>(p, sm, it, local, s_in, s_out);
-      default: return process_unit<W, 4, true>(p, sm, it, local, s_in, s_out);
+      case 0: return process_unit<W, 0, true, false>(p, sm, it, local, s_in, s_out);
+      case 1: return process_unit<W, 1, true, false>(p, sm, it, local, s_in, s_out);
+      default: return process_unit<W, 2, true, false>(p, sm, it, local, s_in, s_out);
     }
   }
   switch (e) {
-    case 0: return process_unit<W, 0, false>(p, sm, it, local, s_in, s_out);
-    case 1: return process_unit<W, 1, false>(p, sm, it, local, s_in, s_out);
-    case 2: return process_unit<W, 2, false>(p, sm, it, local, s_in, s_out);
-    case 3: return process_unit<W, 3, false>(p, sm, it, local, s_in, s_out);
-    default: return process_unit<W, 4, false>(p, sm, it, local, s_in, s_out);
+    case 0: return process_unit<W, 0, false, false>(p, sm, it, local, s_in, s_out);
+    case 1: return process_unit<W, 1, false, false>(p, sm, it, local, s_in, s_out);
+    default: return process_unit<W, 2, false, false>(p, sm, it, local, s_in, s_out);
   }
 }
 
@@ -498,7 +567,9 @@ __global__ void __launch_bounds__(kThreads) spine_kernel(Params<W> p) {
   __syncthreads();
   for (;;) {
     if (threadIdx.x == 0) {
+      const unsigned long long stride = p.unit_stride ? p.unit_stride : 1ULL;
       unsigned long long u = atomicAdd(p.counter, 1ULL);
+      u = u < p.total_units ? u * stride + p.unit_offset : ~0ULL;
       if (u >= p.total_units) u = ~0ULL;
       if (u != ~0ULL && p.budget_ns && globaltimer_ns() - *p.start_ns > p.budget_ns) {
         atomicOr(&p.flags[0], 1);
@@ -728,7 +799,7 @@ struct Enumerator {
 // Structural inversion depth: levels are inverted top-down until the first
 // arithmetic level that lies below an & or | (its constraint mask is then
 // not of the form 2^n - 1).
-static inline void finish_item(Item& it, int threads, uint64_t mask) {
+static inline void finish_structure(Item& it, uint64_t mask) {
   int inv = it.depth;
   bool andor = false, full = true;
   for (int l = 0; l < it.depth; ++l) {
@@ -753,7 +824,12 @@ static inline void finish_item(Item& it, int threads, uint64_t mask) {
   for (int l = 0; l < it.depth; ++l)
     if (it.lv[l].kind == 0) nctx *= it.lv[l].nsmall;
   it.nctx = nctx;
-  // thread layout: G groups of kR contexts, L lanes over the values
+}
+
+// Thread layout and work units: G groups of kR contexts x L lanes over the
+// bottom values, about 2^22 candidates per unit.
+static inline void finish_layout(Item& it, int threads) {
+  const uint64_t nctx = it.nctx;
   uint64_t groups = (nctx + kR - 1) / kR;
   int G = 1;
   while (G < threads && (uint64_t)G < groups) G <<= 1;
@@ -769,6 +845,64 @@ static inline void finish_item(Item& it, int threads, uint64_t mask) {
   if (vb > nv_al) vb = nv_al;
   it.vb = vb;
   it.vblocks = (it.nv + vb - 1) / vb;
+}
+
+static inline void finish_item(Item& it, int threads, uint64_t mask) {
+  finish_structure(it, mask);
+  finish_layout(it, threads);
+}
+
+// Fully inverted spines with fewer contexts than one work unit holds would
+// each stream their bottom table once; spines sharing a bottom size (and
+// mask kind) are fused into one context list instead, materialised on the
+// device.  Returns the fused work items; `small` receives the member spines
+// with their offsets into the list.
+static inline void fuse_small(std::vector<Item>& items, std::vector<Item>* small, uint64_t* nctxs,
+                              const CountTable& ct, uint64_t max_ctxs) {
+  std::vector<Item> keep;
+  std::vector<Item> groups;
+  std::vector<std::vector<size_t>> members;
+  uint64_t total = 0;
+  for (auto& it : items) {
+    const bool fusable = it.nexp == 0 && it.nctx < (uint64_t)kThreads * kR && total + it.nctx <= max_ctxs;
+    if (!fusable) {
+      keep.push_back(it);
+      continue;
+    }
+    size_t gi = 0;
+    for (; gi < groups.size(); ++gi)
+      if (groups[gi].bottom == it.bottom && groups[gi].full == it.full) break;
+    if (gi == groups.size()) {
+      Item g;
+      memset(&g, 0, sizeof(g));
+      g.bottom = it.bottom;
+      g.full = it.full;
+      g.fused = 1;
+      g.nv = ct.n[(int)it.bottom][8];
+      g.base = ~0ULL;
+      groups.push_back(g);
+      members.emplace_back();
+    }
+    members[gi].push_back(small->size());
+    groups[gi].base = std::min(groups[gi].base, it.base);
+    groups[gi].nctx += it.nctx;
+    small->push_back(it);
+    total += it.nctx;
+  }
+  uint64_t off = 0;
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    groups[gi].ctx_off = off;
+    for (size_t m : members[gi]) {
+      (*small)[m].ctx_off = off;
+      off += (*small)[m].nctx;
+    }
+    keep.push_back(groups[gi]);
+  }
+  // the materialize kernel finds a context's spine by binary search
+  std::sort(small->begin(), small->end(),
+            [](const Item& a, const Item& b) { return a.ctx_off < b.ctx_off; });
+  *nctxs = off;
+  items.swap(keep);
 }
 
 template <class W>
@@ -853,6 +987,32 @@ class Search final : public SearchSession {
   int solve(int max_size, SolveOutcome* out) override { return run(max_size, 0, 0, true, out); }
   int sweep(int lo, int hi, SolveOutcome* out) override { return run(hi, lo, hi, false, out); }
 
+  // One size over the work units u with u % nshards == shard (the others
+  // belong to other GPUs); the caller combines the shards' minima.
+  int search_one_size(int s, int shard, int nshards, SizeOutcome* out) override {
+    *out = SizeOutcome();
+    if (s < 1 || s > count_ok_max_ || nshards < 1 || shard < 0 || shard >= nshards) {
+      set_last_error("bad size or shard");
+      return SIMBA_E_ARG;
+    }
+    launches_ = 0;
+    kernel_ms_ = 0.0;
+    alg_ops_ = 0;
+    stamp_start_kernel<<<1, 1, 0, stream_>>>(d_scal_.as<unsigned long long>() + 3);
+    ++launches_;
+    SB_CUDA(cudaGetLastError());
+    uint64_t best = ~0ULL;
+    double ms = 0;
+    const int rc = search_size(s, true, &best, &out->evaluated, &ms, shard, nshards);
+    out->best = best;
+    out->candidates = ct_.n[s][8];
+    out->device_ms = ms;
+    out->kernel_ms = kernel_ms_;
+    out->launches = launches_;
+    out->status = rc == SIMBA_BUDGET ? SIMBA_BUDGET : (best != ~0ULL ? SIMBA_OK : SIMBA_NOT_FOUND);
+    return rc < 0 ? rc : out->status;
+  }
+
  private:
   static uint64_t padded(uint64_t n) { return (n + 63) / 64 * 64 + 64; }
 
@@ -932,7 +1092,8 @@ class Search final : public SearchSession {
     return c;
   }
 
-  int search_size(int s, bool stop, uint64_t* best, uint64_t* evaluated, double* ms) {
+  int search_size(int s, bool stop, uint64_t* best, uint64_t* evaluated, double* ms, int shard = 0,
+                  int nshards = 1) {
     double alg_total = 0;
     // reset counter, best, evaluated, flags
     unsigned long long init[8] = {0, ~0ULL, 0, 0, 0, 0, 0, 0};
@@ -968,11 +1129,19 @@ class Search final : public SearchSession {
     if (!use_naive) {
       int rc = ensure_tables(std::min(T, s));
       if (rc) return rc;
-      uint64_t units = 0;
       for (auto& it : items) {
         for (int l = 0; l < it.depth; ++l)
           if (it.lv[l].kind == 1) it.lv[l].c &= mask_;
-        finish_item(it, kThreads, mask_);
+        finish_structure(it, mask_);
+      }
+      std::vector<Item> small;
+      uint64_t nctxs = 0;
+      fuse_small(items, &small, &nctxs, ct_, 1ULL << 22);
+      for (auto& it : items) finish_layout(it, kThreads);
+      std::stable_sort(items.begin(), items.end(),
+                       [](const Item& a, const Item& b) { return a.base < b.base; });
+      uint64_t units = 0;
+      for (auto& it : items) {
         it.unit_begin = units;
         units += it.cblocks * it.vblocks;
       }
@@ -984,8 +1153,23 @@ class Search final : public SearchSession {
       p.items = d_items_.as<Item>();
       p.nitems = (int)items.size();
       p.total_units = units;
+      p.unit_offset = (unsigned long long)shard;
+      p.unit_stride = (unsigned long long)nshards;
       p.stop_on_match = stop ? 1 : 0;
       SB_CUDA(cudaEventRecord(evk_, stream_));
+      if (nctxs) {
+        SB_CUDA(d_small_.reserve(small.size() * sizeof(Item)));
+        SB_CUDA(cudaMemcpyAsync(d_small_.p, small.data(), small.size() * sizeof(Item),
+                                cudaMemcpyHostToDevice, stream_));
+        SB_CUDA(d_ctx_.reserve(nctxs * sizeof(Ctx<W>)));
+        p.sitems = d_small_.as<Item>();
+        p.nsitems = (int)small.size();
+        p.nctxs = nctxs;
+        const int mb = (int)std::min<uint64_t>((nctxs + 255) / 256, (uint64_t)sms_ * 8);
+        materialize_kernel<W><<<mb, 256, 0, stream_>>>(p, d_ctx_.as<Ctx<W>>());
+        ++launches_;
+        p.ctxs = d_ctx_.as<Ctx<W>>();
+      }
       spine_kernel<W><<<grid_, kThreads, smem_bytes_, stream_>>>(p);
       ++launches_;
       SB_CUDA(cudaGetLastError());
@@ -994,7 +1178,10 @@ class Search final : public SearchSession {
       p.stop_on_match = stop ? 1 : 0;
       alg_total = (double)ct_.n[s][8] * (double)s * (sizeof(W) == 8 ? 2.0 : 1.0);
       SB_CUDA(cudaEventRecord(evk_, stream_));
-      naive_kernel<W><<<grid_naive_, kThreads, smem_bytes_, stream_>>>(p, 0, ct_.n[s][8]);
+      const unsigned __int128 n = ct_.n[s][8];
+      const uint64_t lo = (uint64_t)(n * (unsigned)shard / (unsigned)nshards);
+      const uint64_t hi = (uint64_t)(n * (unsigned)(shard + 1) / (unsigned)nshards);
+      naive_kernel<W><<<grid_naive_, kThreads, smem_bytes_, stream_>>>(p, lo, hi);
       ++launches_;
       SB_CUDA(cudaGetLastError());
     }
@@ -1121,7 +1308,7 @@ class Search final : public SearchSession {
   uint64_t alg_ops_ = 0;
   int sms_ = 0, grid_ = 0, grid_naive_ = 0;
   size_t smem_bytes_ = 0;
-  DevBuf d_in_, d_out_, d_counts_, d_scal_, d_tab_, d_items_;
+  DevBuf d_in_, d_out_, d_counts_, d_scal_, d_tab_, d_items_, d_small_, d_ctx_;
   void* h_scal_ = nullptr;
   uint64_t tab_off_[kMaxSize + 1] = {};
   int Tcap_ = 0, built_ = 0, last_T_ = 0;
