@@ -41,7 +41,8 @@ typedef struct {
   int32_t num_variables;
   int32_t num_examples;
   int32_t word_bits;
-  int32_t reserved;
+  int32_t unit_log2;     /* batch only: work-unit size chosen by the autotuner
+                            for this instance's bucket, 0 = opt->unit_log2   */
   const uint64_t *inputs;
   const uint64_t *outputs;
 } simba_instance;
@@ -60,7 +61,9 @@ typedef struct {
                             (max pitch / (4 * samples), full-cache.cu:713-718)  */
   int32_t vfb_reference_dedup; /* 1: VFB keeps the reference's uniqueness test
                             as written (stores repeated vectors)                */
-  int32_t reserved[3];
+  int32_t unit_log2;     /* log2 of candidates per work unit, 0 = 22 (autotuned
+                            per bucket by the Python autotuner)                  */
+  int32_t reserved[2];
 } simba_options;
 
 typedef struct {
@@ -131,6 +134,41 @@ int vfb_solve(const simba_instance *inst, int max_len, const simba_options *opt,
  * or event and reports only host-clock seconds. */
 int simba_solve_noalloc(const simba_instance *inst, int max_size, const simba_options *opt,
                         simba_result *result);
+
+/* Per-instance result of a batch. */
+typedef struct {
+  int32_t status;
+  int32_t size;
+  int32_t op;
+  int32_t reserved;
+  uint64_t rank;
+  char postfix[64];
+  double seconds;        /* time to solution, from the start of the batch        */
+  uint64_t candidates;   /* reference-rule candidates of this instance           */
+} simba_batch_result;
+
+typedef struct {
+  double seconds;
+  double device_ms;
+  double kernel_ms;      /* spine / build kernels of all rounds                  */
+  double alg_ops;        /* integer lane-operations of the candidates evaluated  */
+  uint64_t candidates;
+  uint64_t evaluated;
+  int32_t rounds;        /* one persistent launch per round (size step)          */
+  int32_t launches;
+  int32_t solved;
+  int32_t reserved;
+} simba_batch_stats;
+
+/* Batched plain search of n independent instances of one word width (no
+ * counterpart in the reference, which runs one process per instance,
+ * run_all.sh:20-43).  Instances advance size by size in rounds; each round
+ * is one persistent kernel whose work queue spans every active instance, and
+ * an instance whose size produced a match retires at the end of the round.
+ * opt->table_bytes caps each instance's value tables (0 = 8 MiB);
+ * opt->budget_seconds bounds the whole batch. */
+int simba_solve_batch(const simba_instance *insts, int n, int max_size, const simba_options *opt,
+                      simba_batch_result *results, simba_batch_stats *stats);
 
 /* Resident session: samples and value tables stay on the device between
  * calls (used by the benchmark to time the search with inputs in HBM). */

@@ -34,7 +34,7 @@ class SimbaError(RuntimeError):
 
 class _Instance(C.Structure):
     _fields_ = [("num_variables", C.c_int32), ("num_examples", C.c_int32),
-                ("word_bits", C.c_int32), ("reserved", C.c_int32),
+                ("word_bits", C.c_int32), ("unit_log2", C.c_int32),
                 ("inputs", C.POINTER(C.c_uint64)), ("outputs", C.POINTER(C.c_uint64))]
 
 
@@ -43,7 +43,20 @@ class _Options(C.Structure):
                 ("engine", C.c_int32), ("budget_seconds", C.c_double),
                 ("table_bytes", C.c_int64), ("stream", C.c_uint64),
                 ("vfb_cache_rows", C.c_int64), ("vfb_reference_dedup", C.c_int32),
-                ("reserved", C.c_int32 * 3)]
+                ("unit_log2", C.c_int32), ("reserved", C.c_int32 * 2)]
+
+
+class _BatchResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("size", C.c_int32), ("op", C.c_int32),
+                ("reserved", C.c_int32), ("rank", C.c_uint64), ("postfix", C.c_char * 64),
+                ("seconds", C.c_double), ("candidates", C.c_uint64)]
+
+
+class _BatchStats(C.Structure):
+    _fields_ = [("seconds", C.c_double), ("device_ms", C.c_double), ("kernel_ms", C.c_double),
+                ("alg_ops", C.c_double), ("candidates", C.c_uint64), ("evaluated", C.c_uint64),
+                ("rounds", C.c_int32), ("launches", C.c_int32), ("solved", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class _SizeResult(C.Structure):
@@ -103,6 +116,8 @@ def lib():
     L.simba_int_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
     L.vfb_solve.argtypes = [P(_Instance), C.c_int, P(_Options), P(_VfbResult)]
     L.simba_solve_noalloc.argtypes = [P(_Instance), C.c_int, P(_Options), P(_Result)]
+    L.simba_solve_batch.argtypes = [P(_Instance), C.c_int, C.c_int, P(_Options),
+                                    P(_BatchResult), P(_BatchStats)]
     L.simba_session_search_size.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int,
                                             P(_SizeResult)]
     _lib = L
@@ -145,13 +160,15 @@ class _Arrays:
     def __init__(self, inst: Instance):
         self.ins = np.ascontiguousarray(inst.inputs, dtype=np.uint64).reshape(-1)
         self.outs = np.ascontiguousarray(inst.outputs, dtype=np.uint64).reshape(-1)
-        self.c = _Instance(inst.num_variables, inst.num_examples, inst.word_bits, 0,
+        self.c = _Instance(inst.num_variables, inst.num_examples, inst.word_bits,
+                           int(getattr(inst, "unit_log2", 0) or 0),
                            self.ins.ctypes.data_as(C.POINTER(C.c_uint64)),
                            self.outs.ctypes.data_as(C.POINTER(C.c_uint64)))
 
 
 def _opts(device=0, complete=False, verbose=False, naive=False, budget=0.0,
-          table_bytes=0, stream=0, cache_rows=0, reference_dedup=False) -> _Options:
+          table_bytes=0, stream=0, cache_rows=0, reference_dedup=False,
+          unit_log2=0) -> _Options:
     o = _Options()
     o.device = device
     o.size_range = 1 if complete else 0
@@ -162,6 +179,7 @@ def _opts(device=0, complete=False, verbose=False, naive=False, budget=0.0,
     o.stream = int(stream)
     o.vfb_cache_rows = int(cache_rows)
     o.vfb_reference_dedup = 1 if reference_dedup else 0
+    o.unit_log2 = int(unit_log2)
     return o
 
 
@@ -189,6 +207,28 @@ def solve_noalloc(inst: Instance, max_size: int, **kw) -> Result:
     rc = lib().simba_solve_noalloc(C.byref(a.c), max_size, C.byref(_opts(**kw)), C.byref(r))
     _check(rc)
     return _res(r)
+
+
+def solve_batch(insts: Sequence[Instance], max_size: int, **kw):
+    """Batched plain search: returns (per-instance Result list, stats dict).
+
+    Each Result carries status, size, op, rank, postfix, expr, candidates and
+    `seconds` = time to solution from the start of the batch."""
+    n = len(insts)
+    arrs = [_Arrays(i) for i in insts]
+    carr = (_Instance * n)(*[a.c for a in arrs])
+    res = (_BatchResult * max(n, 1))()
+    st = _BatchStats()
+    _check(lib().simba_solve_batch(carr, n, max_size, C.byref(_opts(**kw)), res, C.byref(st)))
+    out = []
+    for i in range(n):
+        r = res[i]
+        pf = r.postfix.decode()
+        out.append(Result(r.status, r.size, r.op, r.rank, pf,
+                          format_postfix(pf) if r.status == OK else "Not found !",
+                          r.seconds, 0.0, r.candidates))
+    stats = {k: getattr(st, k) for k, _ in _BatchStats._fields_ if k != "reserved"}
+    return out, stats
 
 
 @dataclass

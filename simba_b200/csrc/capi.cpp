@@ -119,6 +119,7 @@ static int to_host(const simba_instance* inst, HostInstance* h) {
   h->k = inst->num_variables;
   h->S = inst->num_examples;
   h->bits = inst->word_bits == 0 ? 32 : inst->word_bits;
+  h->unit_log2 = inst->unit_log2;
   if (h->k < 1 || h->S < 1 || h->k > kMaxTerms || h->S > kMaxSamples) {
     set_last_error("instance limits exceeded");
     return SIMBA_E_ARG;
@@ -141,6 +142,7 @@ static EngineOptions to_opts(const simba_options* o) {
     e.budget_s = o->budget_seconds;
     e.table_bytes = o->table_bytes;
     e.stream = o->stream;
+    e.unit_log2 = o->unit_log2;
   }
   return e;
 }
@@ -296,6 +298,47 @@ int simba_solve_noalloc(const simba_instance* inst, int max_size, const simba_op
   }
   fill_result(oc, secs, result);
   return result->status;
+}
+
+int simba_solve_batch(const simba_instance* insts, int n, const int max_size_arg,
+                      const simba_options* opt, simba_batch_result* results, simba_batch_stats* stats) {
+  if (!insts || n < 0 || !results) return SIMBA_E_ARG;
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<HostInstance> hs(n);
+  for (int i = 0; i < n; ++i) {
+    const int rc = to_host(insts + i, &hs[i]);
+    if (rc) return rc;
+  }
+  BatchOutcome oc;
+  const int rc = batch_solve(hs, max_size_arg, to_opts(opt), opt ? opt->table_bytes : 0, &oc);
+  if (rc < 0) return rc;
+  int solved = 0;
+  for (int i = 0; i < n; ++i) {
+    simba_batch_result& r = results[i];
+    memset(&r, 0, sizeof(r));
+    const BatchItemOutcome& o = oc.items[i];
+    r.status = o.status;
+    r.size = o.size;
+    r.op = o.op;
+    r.rank = o.rank;
+    snprintf(r.postfix, sizeof(r.postfix), "%s", o.postfix.c_str());
+    r.seconds = o.seconds;
+    r.candidates = o.candidates;
+    solved += o.status == SIMBA_OK;
+  }
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    stats->device_ms = oc.device_ms;
+    stats->kernel_ms = oc.kernel_ms;
+    stats->alg_ops = oc.alg_ops;
+    stats->candidates = oc.candidates;
+    stats->evaluated = oc.evaluated;
+    stats->rounds = oc.rounds;
+    stats->launches = oc.launches;
+    stats->solved = solved;
+  }
+  return 0;
 }
 
 int simba_session_create(const simba_instance* inst, const simba_options* opt,

@@ -17,6 +17,7 @@ struct HostInstance {
   int bits = 32;      // 32 or 64
   std::vector<uint64_t> in;   // S*k sample-major
   std::vector<uint64_t> out;  // S
+  int unit_log2 = 0;          // batch: autotuned work-unit size, 0 = options
 };
 
 struct EngineOptions {
@@ -28,6 +29,7 @@ struct EngineOptions {
   int engine = 0;            // 0 spine (auto), 1 naive per-rank kernel
   int stop_on_match = 1;     // 0: evaluate whole sizes (throughput sweeps)
   uint64_t stream = 0;       // caller's cudaStream_t, 0 = own stream
+  int unit_log2 = 0;         // log2 candidates per work unit, 0 = 22
 };
 
 // Per-solve outcome filled by the engines (capi.cpp formats the strings).
@@ -82,6 +84,27 @@ int make_search_session(const HostInstance& h, const EngineOptions& o,
 
 // Plain search with all scratch in a static __device__ array (search_static.cu).
 int solve_static(const HostInstance& h, int max_size, const EngineOptions& o, SolveOutcome* out);
+
+struct BatchItemOutcome {
+  int status = SIMBA_NOT_FOUND;
+  int size = 0, op = -1;
+  uint64_t rank = 0;
+  std::string postfix;
+  double seconds = 0.0;
+  uint64_t candidates = 0;
+};
+
+struct BatchOutcome {
+  std::vector<BatchItemOutcome> items;
+  double device_ms = 0.0, kernel_ms = 0.0, alg_ops = 0.0;
+  int rounds = 0, launches = 0;
+  uint64_t evaluated = 0, candidates = 0;
+};
+
+// Batched plain search of independent instances of one word width
+// (search_impl.cuh: Batch).  inst_table_bytes caps each instance's tables.
+int batch_solve(const std::vector<HostInstance>& hs, int max_size, const EngineOptions& o,
+                int64_t inst_table_bytes, BatchOutcome* out);
 
 // Read an instance file in the reference JSON schema.
 int read_instance_json(const std::string& path, HostInstance* h);

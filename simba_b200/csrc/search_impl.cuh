@@ -38,7 +38,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
+#include <map>
 #include <cstdio>
 #include <cstddef>
 #include <cstring>
@@ -54,7 +56,23 @@ namespace simba {
 constexpr int kMaxDepth = 12;  // spine levels
 constexpr int kThreads = 256;  // CTA size of the search kernels
 constexpr int kQueue = 128;    // shared-memory queue of sample-0 matches
-constexpr int kR = 4;          // contexts per thread
+// Tuning knobs (compile-time): contexts per thread, software pipelining of
+// the bottom-value loads, minimum resident CTAs per SM.
+#ifndef SIMBA_KR
+#define SIMBA_KR 8
+#endif
+#ifndef SIMBA_PIPE
+#define SIMBA_PIPE 0
+#endif
+#ifndef SIMBA_MINB
+#define SIMBA_MINB 0
+#endif
+#if SIMBA_MINB > 0
+#define SIMBA_SPINE_BOUNDS __launch_bounds__(256, SIMBA_MINB)
+#else
+#define SIMBA_SPINE_BOUNDS __launch_bounds__(256)
+#endif
+constexpr int kR = SIMBA_KR;   // contexts per thread
 constexpr int kMaxExplicit = 2;
 
 // One level of a spine, top-down (level 0 is the root).
@@ -85,7 +103,8 @@ struct alignas(16) Item {
   int8_t fused;         // 1: contexts are read from the materialised list
   int8_t pad[2];
   uint64_t ctx_off;     // fused: first context in Params::ctxs
-  uint64_t pad2;
+  uint32_t inst;        // instance (index into Params::insts)
+  uint32_t pad2;
   Level lv[kMaxDepth];
 };
 
@@ -98,19 +117,51 @@ struct Ctx {
 };
 static_assert(sizeof(Item) % 16 == 0, "Item must be 16-byte sized");
 
+// Everything the kernels need about one instance (several per launch in
+// batch mode): value tables, samples, count table, the sample-0 target, the
+// size being searched and where its minimum matching rank accumulates.
+template <class W>
+struct alignas(16) InstDesc {
+  const W* tab[kMaxSize + 1];
+  const W* in;                      // S*K words, 16-byte padded
+  const W* out;                     // S words, 16-byte padded
+  const unsigned long long* counts; // (kMaxSize+1) x kCols count table
+  unsigned long long* best;         // minimum verified matching rank
+  W target;                         // output on sample 0
+  int size;
+  int S, K;
+  int pad[3];
+};
+
+// Batch mode: one instance's search of one size, pointing at a shared spine
+// list (TmplDesc) that lives once on the device for all instances with the
+// same (terminals, tabled size, size, unit size).
+struct Task {
+  unsigned long long unit_begin;  // first global unit of this task
+  unsigned long long ctx_base;    // first materialised context of this task
+  unsigned int inst;
+  unsigned int tmpl;
+};
+
+struct TmplDesc {
+  unsigned long long item_off;    // into Params::items
+  unsigned long long small_off;   // into Params::sitems
+  unsigned int nitems;
+  unsigned int nsmall;
+};
+
 template <class W>
 struct Params {
-  const W* tab[kMaxSize + 1];
+  const InstDesc<W>* insts;
+  const Task* tasks;        // batch mode when non-null
+  const TmplDesc* tmpls;
+  int ntasks;
   const Item* items;
   const Ctx<W>* ctxs;     // materialised contexts of fused groups
   const Item* sitems;     // spines whose contexts are materialised
   int nsitems;
   unsigned long long nctxs;
-  const W* in;
-  const W* out;
-  const unsigned long long* counts;
   unsigned long long* counter;
-  unsigned long long* best;
   unsigned long long* evaluated;
   unsigned long long* start_ns;
   int* flags;  // [0] budget expired, [1] inversion failure, [2] queue overflows
@@ -118,22 +169,26 @@ struct Params {
   unsigned long long unit_offset;  // this shard's first unit (multi-GPU)
   unsigned long long unit_stride;  // number of shards (0 is read as 1)
   unsigned long long budget_ns;
-  W target;
   int nitems;
-  int size;
-  int S, K;
   int stop_on_match;
+  int maxS, maxK;  // largest instance staged in shared memory
 };
 
 struct alignas(16) Smem {
   unsigned long long counts[(kMaxSize + 1) * kCols];
   Item item;  // 16-byte aligned: filled with uint4 copies
+  alignas(16) unsigned char desc[sizeof(InstDesc<unsigned long long>)];
+  int inst_idx;
+  int pad_[3];
   unsigned long long queue[kQueue];
   unsigned long long unit;
+  unsigned long long unit_local;  // unit index within its spine
   int qn;
   int item_idx;
   int next_item;
   int skip;
+  int task_idx;
+  int next_task;
   char post[kThreads / 32][kMaxSize + 8];
 };
 
@@ -270,12 +325,12 @@ __device__ W eval_postfix(const char* p, int len, const W* row) {
 
 // Single-thread verification on every sample (used when the queue is full).
 template <class W>
-__device__ bool thread_verify(const Params<W>& p, const Smem& sm, const W* s_in, const W* s_out,
+__device__ bool thread_verify(const InstDesc<W>& d, const Smem& sm, const W* s_in, const W* s_out,
                               unsigned long long rank) {
   char post[kMaxSize + 1];
-  unrank(rank, p.size, (const uint64_t(*)[kCols])sm.counts, post);
-  for (int i = 0; i < p.S; ++i)
-    if (eval_postfix<W>(post, p.size, s_in + i * p.K) != s_out[i]) return false;
+  unrank(rank, d.size, (const uint64_t(*)[kCols])sm.counts, post);
+  for (int i = 0; i < d.S; ++i)
+    if (eval_postfix<W>(post, d.size, s_in + i * d.K) != s_out[i]) return false;
   return true;
 }
 
@@ -283,26 +338,26 @@ __device__ bool thread_verify(const Params<W>& p, const Smem& sm, const W* s_in,
 // checks samples i, i+32, ...; a ballot after each group of 32 samples
 // rejects the candidate at the first mismatch.
 template <class W>
-__device__ void verify_queue(const Params<W>& p, Smem& sm, const W* s_in, const W* s_out) {
+__device__ void verify_queue(const InstDesc<W>& d, Smem& sm, const W* s_in, const W* s_out) {
   const int nq = min(sm.qn, kQueue);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int h = warp; h < nq; h += kThreads / 32) {
     const unsigned long long rank = sm.queue[h];
     unsigned long long cur = 0;
-    if (lane == 0) cur = *(volatile unsigned long long*)p.best;
+    if (lane == 0) cur = *(volatile unsigned long long*)d.best;
     cur = __shfl_sync(0xffffffffu, cur, 0);
     if (rank >= cur) continue;
     char* post = sm.post[warp];
-    if (lane == 0) unrank(rank, p.size, (const uint64_t(*)[kCols])sm.counts, post);
+    if (lane == 0) unrank(rank, d.size, (const uint64_t(*)[kCols])sm.counts, post);
     __syncwarp();
     bool all_ok = true;
-    for (int base = 0; base < p.S; base += 32) {
+    for (int base = 0; base < d.S; base += 32) {
       const int i = base + lane;
       bool ok = true;
-      if (i < p.S) ok = eval_postfix<W>(post, p.size, s_in + i * p.K) == s_out[i];
+      if (i < d.S) ok = eval_postfix<W>(post, d.size, s_in + i * d.K) == s_out[i];
       if (__ballot_sync(0xffffffffu, !ok)) { all_ok = false; break; }
     }
-    if (all_ok && lane == 0) atomicMin(p.best, rank);
+    if (all_ok && lane == 0) atomicMin(d.best, rank);
     __syncwarp();
   }
 }
@@ -310,7 +365,7 @@ __device__ void verify_queue(const Params<W>& p, Smem& sm, const W* s_in, const 
 // Decode context index c into small-side indices (deepest level fastest)
 // and return its rank base; optionally fetch the small values.
 template <class W>
-__device__ __forceinline__ unsigned long long decode_context(const Params<W>& p, const Item& it,
+__device__ __forceinline__ unsigned long long decode_context(const InstDesc<W>& d, const Item& it,
                                                              unsigned long long c, W* wl) {
   unsigned long long rank = it.base;
   for (int l = it.depth - 1; l >= 0; --l) {
@@ -319,20 +374,20 @@ __device__ __forceinline__ unsigned long long decode_context(const Params<W>& p,
     const unsigned long long idx = c % L.nsmall;
     c /= L.nsmall;
     rank += idx * L.coef;
-    if (wl) wl[l] = p.tab[L.ts][idx];
+    if (wl) wl[l] = d.tab[L.ts][idx];
   }
   return rank;
 }
 
 template <class W>
-__device__ __forceinline__ void push_hit(const Params<W>& p, Smem& sm, const W* s_in,
-                                         const W* s_out, unsigned long long rank) {
+__device__ __forceinline__ void push_hit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
+                                         const W* s_in, const W* s_out, unsigned long long rank) {
   const int i = atomicAdd(&sm.qn, 1);
   if (i < kQueue) {
     sm.queue[i] = rank;
   } else {
     atomicAdd(&p.flags[2], 1);
-    if (thread_verify<W>(p, sm, s_in, s_out, rank)) atomicMin(p.best, rank);
+    if (thread_verify<W>(d, sm, s_in, s_out, rank)) atomicMin(d.best, rank);
   }
 }
 
@@ -355,8 +410,8 @@ __device__ __forceinline__ W eval_explicit(const Explicit<W>& X, const W* w, W x
 // values.  Loads are 16-byte vectors of the bottom table, four in flight per
 // thread.  FUSED units take their contexts from the materialised list.
 template <class W, int E, bool FULL, bool FUSED>
-__device__ void process_unit(const Params<W>& p, Smem& sm, const Item& it, unsigned long long local,
-                             const W* s_in, const W* s_out) {
+__device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm, const Item& it,
+                             unsigned long long local, const W* s_in, const W* s_out) {
   constexpr int VW = 16 / sizeof(W);
   constexpr int EE = E > 0 ? E : 1;
   const unsigned long long cblk = local / it.vblocks;
@@ -390,8 +445,8 @@ __device__ void process_unit(const Params<W>& p, Smem& sm, const Item& it, unsig
       continue;
     }
     W wl[kMaxDepth];
-    decode_context<W>(p, it, c, wl);
-    W m = (W)~W(0), k = p.target;
+    decode_context<W>(d, it, c, wl);
+    W m = (W)~W(0), k = d.target;
     for (int l = 0; l < it.inv; ++l)
       if (!invert_level<W>(it.lv[l], wl[l], m, k)) atomicOr(&p.flags[1], 1);
     M[r] = m;
@@ -402,7 +457,7 @@ __device__ void process_unit(const Params<W>& p, Smem& sm, const Item& it, unsig
     }
   }
 
-  const W* V = p.tab[it.bottom];
+  const W* V = d.tab[it.bottom];
   const unsigned long long v0 = vblk * it.vb;
   const unsigned long long v1 = umin64(v0 + it.vb, it.nv);
   const unsigned long long q0 = v0 / VW, q1 = (v1 + VW - 1) / VW;
@@ -436,9 +491,9 @@ __device__ void process_unit(const Params<W>& p, Smem& sm, const Item& it, unsig
           const Ctx<W> cx = p.ctxs[it.ctx_off + c0 + r];
           rank = cx.base + v * cx.coefv;
         } else {
-          rank = decode_context<W>(p, it, c0 + r, nullptr) + v * it.coefv;
+          rank = decode_context<W>(d, it, c0 + r, nullptr) + v * it.coefv;
         }
-        push_hit<W>(p, sm, s_in, s_out, rank);
+        push_hit<W>(p, d, sm, s_in, s_out, rank);
       }
     }
   };
@@ -446,6 +501,32 @@ __device__ void process_unit(const Params<W>& p, Smem& sm, const Item& it, unsig
   unsigned long long q = q0 + lane;
   const unsigned long long step = (unsigned long long)L;
   if (E == 0) {  // four loads in flight; explicit levels keep one (code size)
+#if SIMBA_PIPE
+    // software pipeline: the next four loads are issued before the current
+    // four values are tested
+    const unsigned long long span = 4 * step;
+    if (q + 3 * step < q1) {
+      uint4 a0 = __ldg(V4 + q), a1 = __ldg(V4 + q + step), a2 = __ldg(V4 + q + 2 * step),
+            a3 = __ldg(V4 + q + 3 * step);
+      q += span;
+      for (; q + 3 * step < q1; q += span) {
+        const uint4 b0 = __ldg(V4 + q), b1 = __ldg(V4 + q + step), b2 = __ldg(V4 + q + 2 * step),
+                    b3 = __ldg(V4 + q + 3 * step);
+        test(a0, q - span);
+        test(a1, q - span + step);
+        test(a2, q - span + 2 * step);
+        test(a3, q - span + 3 * step);
+        a0 = b0;
+        a1 = b1;
+        a2 = b2;
+        a3 = b3;
+      }
+      test(a0, q - span);
+      test(a1, q - span + step);
+      test(a2, q - span + 2 * step);
+      test(a3, q - span + 3 * step);
+    }
+#else
     for (; q + 3 * step < q1; q += 4 * step) {
       const uint4 a0 = __ldg(V4 + q);
       const uint4 a1 = __ldg(V4 + q + step);
@@ -456,6 +537,7 @@ __device__ void process_unit(const Params<W>& p, Smem& sm, const Item& it, unsig
       test(a2, q + 2 * step);
       test(a3, q + 3 * step);
     }
+#endif
   }
   for (; q < q1; q += step) test(__ldg(V4 + q), q);
 }
@@ -467,18 +549,35 @@ __global__ void __launch_bounds__(256) materialize_kernel(Params<W> p, Ctx<W>* o
   for (unsigned long long gi = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; gi < p.nctxs;
        gi += (unsigned long long)gridDim.x * blockDim.x) {
     int lo = 0, hi = p.nsitems - 1;
+    unsigned long long key = gi;
+    int inst = -1;
+    if (p.tasks) {  // batch: the task owning context gi, then its shared list
+      int tl = 0, th = p.ntasks - 1;
+      while (tl < th) {
+        const int mid = (tl + th + 1) >> 1;
+        if (p.tasks[mid].ctx_base <= gi) tl = mid;
+        else th = mid - 1;
+      }
+      const Task tk = p.tasks[tl];
+      const TmplDesc td = p.tmpls[tk.tmpl];
+      key = gi - tk.ctx_base;
+      lo = (int)td.small_off;
+      hi = (int)(td.small_off + td.nsmall) - 1;
+      inst = (int)tk.inst;
+    }
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (p.sitems[mid].ctx_off <= gi) lo = mid;
+      if (p.sitems[mid].ctx_off <= key) lo = mid;
       else hi = mid - 1;
     }
     const Item& it = p.sitems[lo];
-    const unsigned long long c = gi - it.ctx_off;
+    const InstDesc<W>& d = p.insts[inst >= 0 ? inst : (int)it.inst];
+    const unsigned long long c = key - it.ctx_off;
     W wl[kMaxDepth];
     Ctx<W> cx;
-    cx.base = decode_context<W>(p, it, c, wl);
+    cx.base = decode_context<W>(d, it, c, wl);
     cx.coefv = it.coefv;
-    W m = (W)~W(0), k = p.target;
+    W m = (W)~W(0), k = d.target;
     for (int l = 0; l < it.depth; ++l)
       if (!invert_level<W>(it.lv[l], wl[l], m, k)) atomicOr(&p.flags[1], 1);
     cx.M = m;
@@ -490,79 +589,99 @@ __global__ void __launch_bounds__(256) materialize_kernel(Params<W> p, Ctx<W>* o
 // Generic unit for spines with more than kMaxExplicit explicit levels:
 // straightforward bottom-up evaluation of every level, one context at a time.
 template <class W>
-__device__ void process_unit_generic(const Params<W>& p, Smem& sm, const Item& it,
-                                     unsigned long long local, const W* s_in, const W* s_out) {
+__device__ void process_unit_generic(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
+                                     const Item& it, unsigned long long local, const W* s_in,
+                                     const W* s_out) {
   const unsigned long long cblk = local / it.vblocks;
   const unsigned long long vblk = local - cblk * it.vblocks;
   const int L = it.L;
   const int g = threadIdx.x / L, lane = threadIdx.x % L;
   const unsigned long long v0 = vblk * it.vb;
   const unsigned long long v1 = umin64(v0 + it.vb, it.nv);
-  const W* V = p.tab[it.bottom];
+  const W* V = d.tab[it.bottom];
   for (int r = 0; r < kR; ++r) {
     const unsigned long long c = cblk * it.cb + (unsigned long long)g * kR + r;
     if (c >= it.nctx) break;
     W wl[kMaxDepth];
-    const unsigned long long rb = decode_context<W>(p, it, c, wl);
+    const unsigned long long rb = decode_context<W>(d, it, c, wl);
     for (unsigned long long v = v0 + lane; v < v1; v += L) {
       W y = V[v];
       for (int l = it.depth - 1; l >= 0; --l) {
         const Level& Lv = it.lv[l];
         y = level_apply<W>(Lv.kind, Lv.op, Lv.small_left, Lv.eps, (W)Lv.c, wl[l], y);
       }
-      if (y == p.target) push_hit<W>(p, sm, s_in, s_out, rb + v * it.coefv);
+      if (y == d.target) push_hit<W>(p, d, sm, s_in, s_out, rb + v * it.coefv);
     }
   }
 }
 
 template <class W>
-__device__ void dispatch_unit(const Params<W>& p, Smem& sm, const Item& it, unsigned long long local,
-                              const W* s_in, const W* s_out) {
+__device__ void dispatch_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm, const Item& it,
+                              unsigned long long local, const W* s_in, const W* s_out) {
   const int e = it.nexp;
   if (it.fused) {
-    if (it.full) return process_unit<W, 0, true, true>(p, sm, it, local, s_in, s_out);
-    return process_unit<W, 0, false, true>(p, sm, it, local, s_in, s_out);
+    if (it.full) return process_unit<W, 0, true, true>(p, d, sm, it, local, s_in, s_out);
+    return process_unit<W, 0, false, true>(p, d, sm, it, local, s_in, s_out);
   }
-  if (e > kMaxExplicit) return process_unit_generic<W>(p, sm, it, local, s_in, s_out);
+  if (e > kMaxExplicit) return process_unit_generic<W>(p, d, sm, it, local, s_in, s_out);
   if (it.full) {
     switch (e) {
-      case 0: return process_unit<W, 0, true, false>(p, sm, it, local, s_in, s_out);
-      case 1: return process_unit<W, 1, true, false>(p, sm, it, local, s_in, s_out);
-      default: return process_unit<W, 2, true, false>(p, sm, it, local, s_in, s_out);
+      case 0: return process_unit<W, 0, true, false>(p, d, sm, it, local, s_in, s_out);
+      case 1: return process_unit<W, 1, true, false>(p, d, sm, it, local, s_in, s_out);
+      default: return process_unit<W, 2, true, false>(p, d, sm, it, local, s_in, s_out);
     }
   }
   switch (e) {
-    case 0: return process_unit<W, 0, false, false>(p, sm, it, local, s_in, s_out);
-    case 1: return process_unit<W, 1, false, false>(p, sm, it, local, s_in, s_out);
-    default: return process_unit<W, 2, false, false>(p, sm, it, local, s_in, s_out);
+    case 0: return process_unit<W, 0, false, false>(p, d, sm, it, local, s_in, s_out);
+    case 1: return process_unit<W, 1, false, false>(p, d, sm, it, local, s_in, s_out);
+    default: return process_unit<W, 2, false, false>(p, d, sm, it, local, s_in, s_out);
   }
 }
 
+// Stage one instance's count table and samples into shared memory
+// (16-byte vector copies; the device arrays are padded to 16 bytes) and
+// return where its outputs start.
 template <class W>
-__device__ void stage_samples(const Params<W>& p, Smem& sm, W* s_in, W* s_out) {
-  for (int i = threadIdx.x; i < (kMaxSize + 1) * kCols; i += blockDim.x) sm.counts[i] = p.counts[i];
-  // 16-byte vector copies; the device arrays are padded to 16 bytes.
-  const int nin = (p.S * p.K * (int)sizeof(W) + 15) / 16;
-  const int nout = (p.S * (int)sizeof(W) + 15) / 16;
-  const uint4* gi = reinterpret_cast<const uint4*>(p.in);
-  const uint4* go = reinterpret_cast<const uint4*>(p.out);
+__device__ W* stage_samples(const InstDesc<W>& d, Smem& sm, W* s_in) {
+  for (int i = threadIdx.x; i < (kMaxSize + 1) * kCols; i += blockDim.x) sm.counts[i] = d.counts[i];
+  const int nin = (d.S * d.K * (int)sizeof(W) + 15) / 16;
+  const int nout = (d.S * (int)sizeof(W) + 15) / 16;
+  W* s_out = s_in + nin * (16 / (int)sizeof(W));
+  const uint4* gi = reinterpret_cast<const uint4*>(d.in);
+  const uint4* go = reinterpret_cast<const uint4*>(d.out);
   uint4* si = reinterpret_cast<uint4*>(s_in);
   uint4* so = reinterpret_cast<uint4*>(s_out);
   for (int i = threadIdx.x; i < nin; i += blockDim.x) si[i] = gi[i];
   for (int i = threadIdx.x; i < nout; i += blockDim.x) so[i] = go[i];
+  return s_out;
+}
+
+// Copy instance `idx`'s descriptor into shared memory and stage its samples
+// (all threads call it; ends with a barrier).
+template <class W>
+__device__ W* load_instance(const Params<W>& p, Smem& sm, int idx, W* s_in) {
+  const uint4* src = reinterpret_cast<const uint4*>(p.insts + idx);
+  uint4* dst = reinterpret_cast<uint4*>(sm.desc);
+  for (int i = threadIdx.x; i < (int)(sizeof(InstDesc<W>) / 16); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  W* s_out = stage_samples<W>(*reinterpret_cast<const InstDesc<W>*>(sm.desc), sm, s_in);
+  __syncthreads();
+  return s_out;
 }
 
 // Persistent search kernel: CTAs take work units from an atomic counter.
 template <class W>
-__global__ void __launch_bounds__(kThreads) spine_kernel(Params<W> p) {
+__global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
   W* s_in = reinterpret_cast<W*>(smem_raw + ((sizeof(Smem) + 15) & ~size_t(15)));
-  W* s_out = s_in + ((p.S * p.K * (int)sizeof(W) + 15) / 16) * (16 / (int)sizeof(W));
-  stage_samples<W>(p, sm, s_in, s_out);
+  W* s_out = s_in;
+  const InstDesc<W>& d = *reinterpret_cast<const InstDesc<W>*>(sm.desc);
   if (threadIdx.x == 0) {
     sm.qn = 0;
     sm.item_idx = -1;
+    sm.task_idx = -2;
+    sm.inst_idx = -1;
   }
   __syncthreads();
   for (;;) {
@@ -577,30 +696,61 @@ __global__ void __launch_bounds__(kThreads) spine_kernel(Params<W> p) {
       }
       sm.unit = u;
       if (u != ~0ULL) {
-        int lo = 0, hi = p.nitems - 1;
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (p.items[mid].unit_begin <= u) lo = mid;
-          else hi = mid - 1;
+        unsigned long long local = u;
+        int ilo = 0, ihi = p.nitems - 1, inst = -1, task = -1;
+        if (p.tasks) {  // batch: task, then the spine inside its shared list
+          int lo = 0, hi = p.ntasks - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (p.tasks[mid].unit_begin <= u) lo = mid;
+            else hi = mid - 1;
+          }
+          task = lo;
+          const Task tk = p.tasks[lo];
+          const TmplDesc td = p.tmpls[tk.tmpl];
+          local = u - tk.unit_begin;
+          ilo = (int)td.item_off;
+          ihi = (int)(td.item_off + td.nitems) - 1;
+          inst = (int)tk.inst;
         }
-        sm.next_item = lo;
-        sm.skip = p.stop_on_match && p.items[lo].base > *(volatile unsigned long long*)p.best;
+        while (ilo < ihi) {
+          const int mid = (ilo + ihi + 1) >> 1;
+          if (p.items[mid].unit_begin <= local) ilo = mid;
+          else ihi = mid - 1;
+        }
+        sm.next_item = ilo;
+        sm.next_task = task;
+        sm.unit_local = local - p.items[ilo].unit_begin;
+        const Item& nx = p.items[ilo];
+        if (inst < 0) inst = (int)nx.inst;
+        sm.skip = p.stop_on_match && nx.base > *(volatile unsigned long long*)p.insts[inst].best;
       }
     }
     __syncthreads();
     const unsigned long long u = sm.unit;
     if (u == ~0ULL) break;
     const int ni = sm.next_item;
-    if (ni != sm.item_idx) {
+    const int nt = sm.next_task;
+    if (ni != sm.item_idx || nt != sm.task_idx) {
       const uint4* src = reinterpret_cast<const uint4*>(p.items + ni);
       uint4* dst = reinterpret_cast<uint4*>(&sm.item);
       for (int i = threadIdx.x; i < (int)(sizeof(Item) / 16); i += blockDim.x) dst[i] = src[i];
+      __syncthreads();
+      if (threadIdx.x == 0 && nt >= 0) {
+        const Task tk = p.tasks[nt];
+        sm.item.inst = tk.inst;
+        if (sm.item.fused) sm.item.ctx_off += tk.ctx_base;
+      }
     }
     __syncthreads();
     if (!sm.skip) {
       const Item& it = sm.item;
-      const unsigned long long local = u - it.unit_begin;
-      dispatch_unit<W>(p, sm, it, local, s_in, s_out);
+      if ((int)it.inst != sm.inst_idx) {  // uniform: every thread reads the same values
+        s_out = load_instance<W>(p, sm, (int)it.inst, s_in);
+        if (threadIdx.x == 0) sm.inst_idx = (int)it.inst;
+      }
+      const unsigned long long local = sm.unit_local;
+      dispatch_unit<W>(p, d, sm, it, local, s_in, s_out);
       if (threadIdx.x == 0) {
         const unsigned long long cblk = local / it.vblocks, vblk = local % it.vblocks;
         const unsigned long long c0 = cblk * it.cb, c1 = umin64(c0 + it.cb, it.nctx);
@@ -609,11 +759,12 @@ __global__ void __launch_bounds__(kThreads) spine_kernel(Params<W> p) {
       }
     }
     __syncthreads();
-    if (sm.qn > 0) verify_queue<W>(p, sm, s_in, s_out);
+    if (sm.qn > 0) verify_queue<W>(d, sm, s_in, s_out);
     __syncthreads();
     if (threadIdx.x == 0) {
       sm.qn = 0;
       sm.item_idx = ni;
+      sm.task_idx = nt;
     }
   }
 }
@@ -628,25 +779,24 @@ __global__ void __launch_bounds__(kThreads) naive_kernel(Params<W> p, unsigned l
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
   W* s_in = reinterpret_cast<W*>(smem_raw + ((sizeof(Smem) + 15) & ~size_t(15)));
-  W* s_out = s_in + ((p.S * p.K * (int)sizeof(W) + 15) / 16) * (16 / (int)sizeof(W));
-  stage_samples<W>(p, sm, s_in, s_out);
-  __syncthreads();
+  W* s_out = load_instance<W>(p, sm, 0, s_in);
+  const InstDesc<W>& d = *reinterpret_cast<const InstDesc<W>*>(sm.desc);
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   unsigned long long count = 0;
   char post[kMaxSize + 1];
   for (unsigned long long r = lo + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; r < hi;
        r += stride) {
-    if (p.stop_on_match && r > *(volatile unsigned long long*)p.best) break;
+    if (p.stop_on_match && r > *(volatile unsigned long long*)d.best) break;
     if ((count & 1023) == 0 && p.budget_ns && globaltimer_ns() - *p.start_ns > p.budget_ns) {
       atomicOr(&p.flags[0], 1);
       break;
     }
-    unrank(r, p.size, (const uint64_t(*)[kCols])sm.counts, post);
+    unrank(r, d.size, (const uint64_t(*)[kCols])sm.counts, post);
     ++count;
-    if (eval_postfix<W>(post, p.size, s_in) != s_out[0]) continue;
+    if (eval_postfix<W>(post, d.size, s_in) != s_out[0]) continue;
     bool ok = true;
-    for (int i = 1; i < p.S && ok; ++i) ok = eval_postfix<W>(post, p.size, s_in + i * p.K) == s_out[i];
-    if (ok) atomicMin(p.best, r);
+    for (int i = 1; i < d.S && ok; ++i) ok = eval_postfix<W>(post, d.size, s_in + i * d.K) == s_out[i];
+    if (ok) atomicMin(d.best, r);
   }
   atomicAdd(p.evaluated, count);
 }
@@ -666,6 +816,40 @@ __global__ void build_binary_kernel(W* out, const W* A, const W* B, unsigned lon
        i += (unsigned long long)gridDim.x * blockDim.x) {
     const unsigned long long a = i / nb;
     out[i] = bin_apply<W>(op, A[a], B[i - a * nb]);
+  }
+}
+
+// One table-building job of the batch: a unary (nb = 1, B unused) or binary
+// operator block of one instance's V_t.
+template <class W>
+struct BuildJob {
+  W* out;
+  const W* A;
+  const W* B;
+  unsigned long long na, nb;
+  int op;
+  int pad;
+  unsigned long long begin;  // first global entry of this job
+};
+
+template <class W>
+__global__ void build_batch_kernel(const BuildJob<W>* jobs, int njobs, unsigned long long total) {
+  for (unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (unsigned long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (jobs[mid].begin <= g) lo = mid;
+      else hi = mid - 1;
+    }
+    const BuildJob<W>& j = jobs[lo];
+    const unsigned long long i = g - j.begin;
+    if (is_unary(j.op)) {
+      j.out[i] = un_apply<W>(j.op, j.A[i]);
+    } else {
+      const unsigned long long a = i / j.nb;
+      j.out[i] = bin_apply<W>(j.op, j.A[a], j.B[i - a * j.nb]);
+    }
   }
 }
 
@@ -828,7 +1012,7 @@ static inline void finish_structure(Item& it, uint64_t mask) {
 
 // Thread layout and work units: G groups of kR contexts x L lanes over the
 // bottom values, about 2^22 candidates per unit.
-static inline void finish_layout(Item& it, int threads) {
+static inline void finish_layout(Item& it, int threads, uint64_t unit_target = 1ULL << 22) {
   const uint64_t nctx = it.nctx;
   uint64_t groups = (nctx + kR - 1) / kR;
   int G = 1;
@@ -837,8 +1021,7 @@ static inline void finish_layout(Item& it, int threads) {
   it.L = (uint16_t)(threads / G);
   it.cb = (uint32_t)(G * kR);
   it.cblocks = (nctx + it.cb - 1) / it.cb;
-  const uint64_t target = 1ULL << 22;  // candidates per unit
-  uint64_t vb = target / it.cb;
+  uint64_t vb = unit_target / it.cb;  // about unit_target candidates per unit
   const uint64_t align = 64ULL * it.L;
   vb = std::max<uint64_t>(align, (vb + align - 1) / align * align);
   const uint64_t nv_al = (it.nv + 63) / 64 * 64;
@@ -950,6 +1133,7 @@ class Search final : public SearchSession {
     SB_CUDA(d_counts_.reserve(sizeof(ct_.n)));
     SB_CUDA(cudaMemcpy(d_counts_.p, ct_.n, sizeof(ct_.n), cudaMemcpyHostToDevice));
     SB_CUDA(d_scal_.reserve(256));
+    SB_CUDA(d_insts_.reserve(sizeof(InstDesc<W>)));
     SB_CUDA(cudaHostAlloc(&h_scal_, 256, cudaHostAllocDefault));
     // table budget -> largest tabled size
     const int64_t budget = o_.table_bytes > 0 ? o_.table_bytes : (4LL << 30);
@@ -1055,23 +1239,30 @@ class Search final : public SearchSession {
     return 0;
   }
 
+  // Kernel parameters for size s; uploads the instance descriptor.
   Params<W> params(int s) {
+    InstDesc<W> d;
+    memset(&d, 0, sizeof(d));
+    for (int t = 1; t <= built_; ++t) d.tab[t] = tab(t);
+    d.in = d_in_.as<W>();
+    d.out = d_out_.as<W>();
+    d.counts = d_counts_.as<unsigned long long>();
+    unsigned long long* sc = d_scal_.as<unsigned long long>();
+    d.best = sc + 1;
+    d.target = (W)h_.out[0];
+    d.size = s;
+    d.S = h_.S;
+    d.K = h_.k;
+    cudaMemcpyAsync(d_insts_.p, &d, sizeof(d), cudaMemcpyHostToDevice, stream_);
     Params<W> p;
     memset(&p, 0, sizeof(p));
-    for (int t = 1; t <= built_; ++t) p.tab[t] = tab(t);
-    p.in = d_in_.as<W>();
-    p.out = d_out_.as<W>();
-    p.counts = d_counts_.as<unsigned long long>();
-    unsigned long long* sc = d_scal_.as<unsigned long long>();
+    p.insts = d_insts_.as<InstDesc<W>>();
     p.counter = sc + 0;
-    p.best = sc + 1;
     p.evaluated = sc + 2;
     p.start_ns = sc + 3;
     p.flags = reinterpret_cast<int*>(sc + 4);
-    p.target = (W)h_.out[0];
-    p.size = s;
-    p.S = h_.S;
-    p.K = h_.k;
+    p.maxS = h_.S;
+    p.maxK = h_.k;
     p.budget_ns = o_.budget_s > 0 ? (unsigned long long)(o_.budget_s * 1e9) : 0;
     return p;
   }
@@ -1137,7 +1328,8 @@ class Search final : public SearchSession {
       std::vector<Item> small;
       uint64_t nctxs = 0;
       fuse_small(items, &small, &nctxs, ct_, 1ULL << 22);
-      for (auto& it : items) finish_layout(it, kThreads);
+      const uint64_t unit_target = 1ULL << (o_.unit_log2 > 0 ? std::min(o_.unit_log2, 40) : 22);
+      for (auto& it : items) finish_layout(it, kThreads, unit_target);
       std::stable_sort(items.begin(), items.end(),
                        [](const Item& a, const Item& b) { return a.base < b.base; });
       uint64_t units = 0;
@@ -1308,11 +1500,510 @@ class Search final : public SearchSession {
   uint64_t alg_ops_ = 0;
   int sms_ = 0, grid_ = 0, grid_naive_ = 0;
   size_t smem_bytes_ = 0;
-  DevBuf d_in_, d_out_, d_counts_, d_scal_, d_tab_, d_items_, d_small_, d_ctx_;
+  DevBuf d_in_, d_out_, d_counts_, d_scal_, d_tab_, d_items_, d_small_, d_ctx_, d_insts_;
   void* h_scal_ = nullptr;
   uint64_t tab_off_[kMaxSize + 1] = {};
   int Tcap_ = 0, built_ = 0, last_T_ = 0;
 };
+
+// ------------------------------------------------------------------ batch
+
+// Fused spine list of one (terms, tabled size, size): spine shapes depend
+// only on these, not on an instance's values, so every instance with the
+// same key shares them (contexts are materialised per instance).
+struct ItemTemplate {
+  std::vector<Item> items;   // fused groups + unfused spines (ctx_off relative)
+  std::vector<Item> small;   // fused members (ctx_off relative)
+  uint64_t nctxs = 0;
+  uint64_t units = 0;
+  double alg = 0;            // algorithmic lane-operations of the whole size
+  double cand = 0;           // candidates evaluated for the whole size
+  bool ok = true;            // false: spines too deep, use per-rank kernel
+  int id = -1;               // index of its TmplDesc on the device
+};
+
+// Batched plain search: many independent instances advance size by size in
+// rounds; one persistent spine_kernel launch per round serves the work
+// units of every active instance (an atomic work queue across instances),
+// and an instance whose size produced a match retires at the end of that
+// round.  Value tables are per instance, built by one batched launch per
+// round.  All instances share the word width W.
+template <class W>
+class Batch {
+ public:
+  struct Out {
+    int status = SIMBA_NOT_FOUND;
+    int size = 0, op = -1;
+    uint64_t rank = 0;
+    std::string postfix;
+    double seconds = 0;
+    uint64_t candidates = 0;
+  };
+
+  Batch(const std::vector<HostInstance>& hs, const EngineOptions& o, int64_t inst_table_bytes,
+        uint64_t unit_target)
+      : hs_(hs), o_(o), inst_budget_(inst_table_bytes), unit_target_(unit_target) {}
+  ~Batch() {
+    if (stream_ && own_stream_) cudaStreamDestroy(stream_);
+    if (e0_) cudaEventDestroy(e0_);
+    if (e1_) cudaEventDestroy(e1_);
+  }
+
+  int run(int max_size, std::vector<Out>* outs, double* device_ms, int* rounds, int* launches,
+          uint64_t* evaluated, uint64_t* candidates, double* alg_ops, double* kernel_ms) {
+    const int n = (int)hs_.size();
+    outs->assign(n, Out());
+    SB_CUDA(cudaSetDevice(o_.device));
+    if (o_.stream) {
+      stream_ = reinterpret_cast<cudaStream_t>(o_.stream);
+      own_stream_ = false;
+    } else {
+      SB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    }
+    SB_CUDA(cudaEventCreate(&e0_));
+    SB_CUDA(cudaEventCreate(&e1_));
+    int sms = 0;
+    SB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, o_.device));
+    const uint64_t mask = sizeof(W) == 8 ? ~0ULL : 0xFFFFFFFFULL;
+    // count tables per distinct terminal count
+    int maxS = 1, maxK = 1;
+    std::vector<int> ct_of(n);
+    for (int i = 0; i < n; ++i) {
+      maxS = std::max(maxS, hs_[i].S);
+      maxK = std::max(maxK, hs_[i].k);
+      int j = 0;
+      for (; j < (int)cts_.size(); ++j)
+        if (cts_[j].terms == hs_[i].k) break;
+      if (j == (int)cts_.size()) {
+        CountTable t;
+        int ms = kMaxSize;
+        while (ms > 1 && !build_count_table(ms, hs_[i].k, &t)) --ms;
+        build_count_table(ms, hs_[i].k, &t);
+        cts_.push_back(t);
+      }
+      ct_of[i] = j;
+    }
+    for (auto& t : cts_)
+      if (max_size > t.max_size) {
+        set_last_error("candidate counts exceed 64 bits at this size");
+        return SIMBA_E_OVERFLOW;
+      }
+    // per-instance tabled size and device layout
+    std::vector<int> T(n);
+    std::vector<uint64_t> tab_off(n), in_off(n), out_off(n);
+    std::vector<std::array<uint64_t, kMaxSize + 1>> toff(n);
+    uint64_t tab_total = 0, smp_total = 0;
+    auto padded = [](uint64_t x) { return (x + 63) / 64 * 64 + 64; };
+    for (int i = 0; i < n; ++i) {
+      const CountTable& ct = cts_[ct_of[i]];
+      uint64_t tot = 0;
+      T[i] = 0;
+      for (int t = 1; t <= ct.max_size && t <= 16; ++t) {
+        const uint64_t b = padded(ct.n[t][8]) * sizeof(W);
+        if (t > 1 && tot + b > (uint64_t)inst_budget_) break;
+        toff[i][t] = tot;
+        tot += b;
+        T[i] = t;
+      }
+      tab_off[i] = tab_total;
+      tab_total += tot;
+      in_off[i] = smp_total;
+      smp_total += ((uint64_t)hs_[i].S * hs_[i].k * sizeof(W) + 15) / 16 * 16;
+      out_off[i] = smp_total;
+      smp_total += ((uint64_t)hs_[i].S * sizeof(W) + 15) / 16 * 16;
+    }
+    SB_CUDA(d_tab_.reserve(tab_total + 256));
+    SB_CUDA(d_smp_.reserve(smp_total + 256));
+    SB_CUDA(d_cts_.reserve(cts_.size() * sizeof(cts_[0].n)));
+    SB_CUDA(d_best_.reserve((size_t)n * 8));
+    SB_CUDA(d_desc_.reserve((size_t)n * sizeof(InstDesc<W>)));
+    SB_CUDA(d_scal_.reserve(256));
+    {
+      std::vector<unsigned char> smp(smp_total, 0);
+      for (int i = 0; i < n; ++i) {
+        W* a = reinterpret_cast<W*>(smp.data() + in_off[i]);
+        W* b = reinterpret_cast<W*>(smp.data() + out_off[i]);
+        for (size_t q = 0; q < hs_[i].in.size(); ++q) a[q] = (W)hs_[i].in[q];
+        for (size_t q = 0; q < hs_[i].out.size(); ++q) b[q] = (W)hs_[i].out[q];
+      }
+      SB_CUDA(cudaMemcpy(d_smp_.p, smp.data(), smp_total, cudaMemcpyHostToDevice));
+      std::vector<uint64_t> cta(cts_.size() * (kMaxSize + 1) * kCols);
+      for (size_t j = 0; j < cts_.size(); ++j)
+        memcpy(cta.data() + j * (kMaxSize + 1) * kCols, cts_[j].n, sizeof(cts_[j].n));
+      SB_CUDA(cudaMemcpy(d_cts_.p, cta.data(), cta.size() * 8, cudaMemcpyHostToDevice));
+      // V_1 of every instance: the terminals on sample 0
+      std::vector<W> v1;
+      for (int i = 0; i < n; ++i) {
+        v1.assign(padded(hs_[i].k), 0);
+        for (int j = 0; j < hs_[i].k; ++j) v1[j] = (W)hs_[i].in[j];
+        SB_CUDA(cudaMemcpyAsync(d_tab_.as<char>() + tab_off[i] + toff[i][1], v1.data(),
+                                v1.size() * sizeof(W), cudaMemcpyHostToDevice, stream_));
+        SB_CUDA(cudaStreamSynchronize(stream_));
+      }
+    }
+    std::vector<int> size(n), built(n, 1);
+    const int first = o_.size_range ? 1 : 2;
+    const int last = o_.size_range ? max_size : max_size - 1;
+    for (int i = 0; i < n; ++i) size[i] = first;
+    std::vector<char> active(n, 1);
+    if (first > last)
+      for (int i = 0; i < n; ++i) active[i] = 0, (*outs)[i].status = SIMBA_NOT_FOUND;
+    auto tabp = [&](int i, int t) {
+      return reinterpret_cast<const W*>(d_tab_.as<char>() + tab_off[i] + toff[i][t]);
+    };
+    const size_t smem = ((sizeof(Smem) + 15) & ~size_t(15)) +
+                        (((size_t)maxS * maxK * sizeof(W) + 15) / 16 + ((size_t)maxS * sizeof(W) + 15) / 16) * 16;
+    SB_CUDA(cudaFuncSetAttribute(spine_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SB_CUDA(cudaFuncSetAttribute(naive_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 1;
+    SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, spine_kernel<W>, kThreads, smem));
+    const int grid = sms * std::max(occ, 1);
+    const auto t0 = std::chrono::steady_clock::now();
+    SB_CUDA(cudaEventRecord(e0_, stream_));
+    stamp_start_kernel<<<1, 1, 0, stream_>>>(d_scal_.as<unsigned long long>() + 3);
+    *launches = 1;
+    *rounds = 0;
+    *evaluated = 0;
+    *candidates = 0;
+    *alg_ops = 0;
+    *kernel_ms = 0;
+    std::vector<InstDesc<W>> desc(n);
+    std::vector<unsigned long long> best(n);
+    for (;;) {
+      bool any = false;
+      for (int i = 0; i < n; ++i) any |= active[i] != 0;
+      if (!any) break;
+      const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      if (o_.budget_s > 0 && el > o_.budget_s) {
+        for (int i = 0; i < n; ++i)
+          if (active[i]) {
+            active[i] = 0;
+            (*outs)[i].status = SIMBA_BUDGET;
+            (*outs)[i].seconds = el;
+          }
+        break;
+      }
+      ++*rounds;
+      // 1. value tables: instances whose current size is tabled build it now
+      build_jobs_.clear();
+      for (int i = 0; i < n; ++i) {
+        if (!active[i]) continue;
+        const int want = std::min(size[i], T[i]);
+        const CountTable& ct = cts_[ct_of[i]];
+        for (int t = built[i] + 1; t <= want; ++t) {
+          uint64_t off = 0;
+          const int sub = t - 1;
+          W* o = const_cast<W*>(tabp(i, t));
+          for (int op = 0; op < 8; ++op) {
+            if (is_unary(op)) {
+              build_jobs_.push_back({o + off, tabp(i, sub), nullptr, ct.n[sub][8], 1, op, 0});
+              off += ct.n[sub][8];
+              continue;
+            }
+            const int fmax = is_commutative(op) ? sub / 2 : sub - 1;
+            for (int f = 1; f <= fmax; ++f) {
+              const uint64_t na = ct.n[f][8], nb = ct.n[sub - f][8];
+              build_jobs_.push_back({o + off, tabp(i, f), tabp(i, sub - f), na, nb, op, 0});
+              off += na * nb;
+            }
+          }
+          built[i] = t;
+        }
+      }
+      if (!build_jobs_.empty()) {
+        uint64_t acc = 0;
+        for (auto& j : build_jobs_) {
+          j.begin = acc;
+          acc += j.na * j.nb;
+        }
+        SB_CUDA(d_jobs_.reserve(build_jobs_.size() * sizeof(BuildJob<W>)));
+        SB_CUDA(cudaMemcpyAsync(d_jobs_.p, build_jobs_.data(), build_jobs_.size() * sizeof(BuildJob<W>),
+                                cudaMemcpyHostToDevice, stream_));
+        const int blocks = (int)std::min<uint64_t>((acc + 255) / 256, (uint64_t)sms * 16);
+        build_batch_kernel<W><<<blocks, 256, 0, stream_>>>(d_jobs_.as<BuildJob<W>>(),
+                                                          (int)build_jobs_.size(), acc);
+        ++*launches;
+        SB_CUDA(cudaGetLastError());
+      }
+      // 2. one task per active instance, pointing at its shared spine list
+      tasks_.clear();
+      uint64_t ctx_base = 0, units = 0;
+      std::vector<int> naive_insts;
+      for (int i = 0; i < n; ++i) {
+        if (!active[i]) continue;
+        const CountTable& ct = cts_[ct_of[i]];
+        const int ul = hs_[i].unit_log2 > 0 ? std::min(hs_[i].unit_log2, 40) : 0;
+        const ItemTemplate& tp =
+            get_template(ct, std::min(T[i], size[i]), size[i], mask, ul ? 1ULL << ul : unit_target_);
+        if (!tp.ok || tp.units == 0) {
+          naive_insts.push_back(i);
+          continue;
+        }
+        Task tk;
+        tk.unit_begin = units;
+        tk.ctx_base = ctx_base;
+        tk.inst = (unsigned)i;
+        tk.tmpl = (unsigned)tp.id;
+        tasks_.push_back(tk);
+        units += tp.units;
+        ctx_base += tp.nctxs;
+        *alg_ops += tp.alg;
+      }
+      if (tmpl_dirty_) {  // upload the spine lists created since the last round
+        SB_CUDA(d_items_.reserve(std::max<size_t>(1, all_items_.size()) * sizeof(Item)));
+        SB_CUDA(cudaMemcpyAsync(d_items_.p, all_items_.data(), all_items_.size() * sizeof(Item),
+                                cudaMemcpyHostToDevice, stream_));
+        SB_CUDA(d_small_.reserve(std::max<size_t>(1, all_small_.size()) * sizeof(Item)));
+        SB_CUDA(cudaMemcpyAsync(d_small_.p, all_small_.data(), all_small_.size() * sizeof(Item),
+                                cudaMemcpyHostToDevice, stream_));
+        SB_CUDA(d_tdesc_.reserve(std::max<size_t>(1, tdescs_.size()) * sizeof(TmplDesc)));
+        SB_CUDA(cudaMemcpyAsync(d_tdesc_.p, tdescs_.data(), tdescs_.size() * sizeof(TmplDesc),
+                                cudaMemcpyHostToDevice, stream_));
+        tmpl_dirty_ = false;
+      }
+      // 3. descriptors and per-instance best
+      for (int i = 0; i < n; ++i) {
+        InstDesc<W>& d = desc[i];
+        memset(&d, 0, sizeof(d));
+        for (int t = 1; t <= built[i]; ++t) d.tab[t] = tabp(i, t);
+        d.in = reinterpret_cast<const W*>(d_smp_.as<char>() + in_off[i]);
+        d.out = reinterpret_cast<const W*>(d_smp_.as<char>() + out_off[i]);
+        d.counts = d_cts_.as<unsigned long long>() + (size_t)ct_of[i] * (kMaxSize + 1) * kCols;
+        d.best = d_best_.as<unsigned long long>() + i;
+        d.target = (W)hs_[i].out[0];
+        d.size = size[i];
+        d.S = hs_[i].S;
+        d.K = hs_[i].k;
+      }
+      SB_CUDA(cudaMemcpyAsync(d_desc_.p, desc.data(), n * sizeof(InstDesc<W>), cudaMemcpyHostToDevice, stream_));
+      SB_CUDA(cudaMemsetAsync(d_best_.p, 0xFF, (size_t)n * 8, stream_));
+      unsigned long long init[3] = {0, 0, 0};
+      SB_CUDA(cudaMemcpyAsync(d_scal_.p, init, sizeof(init), cudaMemcpyHostToDevice, stream_));
+      SB_CUDA(cudaMemsetAsync(d_scal_.as<unsigned long long>() + 4, 0, 32, stream_));
+      Params<W> p;
+      memset(&p, 0, sizeof(p));
+      p.insts = d_desc_.as<InstDesc<W>>();
+      unsigned long long* sc = d_scal_.as<unsigned long long>();
+      p.counter = sc + 0;
+      p.evaluated = sc + 2;
+      p.start_ns = sc + 3;
+      p.flags = reinterpret_cast<int*>(sc + 4);
+      p.maxS = maxS;
+      p.maxK = maxK;
+      p.stop_on_match = 1;
+      p.budget_ns = o_.budget_s > 0 ? (unsigned long long)(o_.budget_s * 1e9) : 0;
+      cudaEvent_t k0 = e1_;
+      (void)k0;
+      float kms = 0;
+      cudaEvent_t ka, kb;
+      SB_CUDA(cudaEventCreate(&ka));
+      SB_CUDA(cudaEventCreate(&kb));
+      SB_CUDA(cudaEventRecord(ka, stream_));
+      if (!tasks_.empty()) {
+        SB_CUDA(d_tasks_.reserve(tasks_.size() * sizeof(Task)));
+        SB_CUDA(cudaMemcpyAsync(d_tasks_.p, tasks_.data(), tasks_.size() * sizeof(Task),
+                                cudaMemcpyHostToDevice, stream_));
+        p.tasks = d_tasks_.as<Task>();
+        p.ntasks = (int)tasks_.size();
+        p.tmpls = d_tdesc_.as<TmplDesc>();
+        p.items = d_items_.as<Item>();
+        p.nitems = (int)all_items_.size();
+        p.total_units = units;
+        if (ctx_base) {
+          SB_CUDA(d_ctx_.reserve(ctx_base * sizeof(Ctx<W>)));
+          p.sitems = d_small_.as<Item>();
+          p.nsitems = (int)all_small_.size();
+          p.nctxs = ctx_base;
+          const int mb = (int)std::min<uint64_t>((ctx_base + 255) / 256, (uint64_t)sms * 8);
+          materialize_kernel<W><<<mb, 256, 0, stream_>>>(p, d_ctx_.as<Ctx<W>>());
+          ++*launches;
+          p.ctxs = d_ctx_.as<Ctx<W>>();
+        }
+        spine_kernel<W><<<grid, kThreads, smem, stream_>>>(p);
+        ++*launches;
+        SB_CUDA(cudaGetLastError());
+      }
+      for (int i : naive_insts) {  // spines too deep for this instance's tables
+        Params<W> q = p;
+        q.tasks = nullptr;
+        q.insts = d_desc_.as<InstDesc<W>>() + i;
+        const CountTable& ct = cts_[ct_of[i]];
+        naive_kernel<W><<<grid, kThreads, smem, stream_>>>(q, 0, ct.n[size[i]][8]);
+        ++*launches;
+        SB_CUDA(cudaGetLastError());
+      }
+      SB_CUDA(cudaEventRecord(kb, stream_));
+      SB_CUDA(cudaMemcpyAsync(best.data(), d_best_.p, (size_t)n * 8, cudaMemcpyDeviceToHost, stream_));
+      unsigned long long hs[8];
+      SB_CUDA(cudaMemcpyAsync(hs, d_scal_.p, sizeof(hs), cudaMemcpyDeviceToHost, stream_));
+      SB_CUDA(cudaStreamSynchronize(stream_));
+      SB_CUDA(cudaEventElapsedTime(&kms, ka, kb));
+      cudaEventDestroy(ka);
+      cudaEventDestroy(kb);
+      *kernel_ms += kms;
+      *evaluated += hs[2];
+      const int* fl = reinterpret_cast<const int*>(hs + 4);
+      if (fl[1]) {
+        set_last_error("inversion failed on a level marked invertible");
+        return SIMBA_E_INTERNAL;
+      }
+      const double now = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      // 4. retire solved instances, advance the others
+      for (int i = 0; i < n; ++i) {
+        if (!active[i]) continue;
+        Out& r = (*outs)[i];
+        const CountTable& ct = cts_[ct_of[i]];
+        const int s = size[i];
+        if (best[i] != ~0ULL) {
+          const int op = s == 1 ? 8 : op_of_rank(ct.n, s, best[i]);
+          uint64_t c = 0;
+          if (s == 1) c = best[i] + 1;
+          else
+            for (int q = 0; q <= op; ++q) c += ct.n[s][q];
+          r.candidates += c;
+          char buf[kMaxSize + 1];
+          unrank(best[i], s, ct.n, buf);
+          buf[s] = 0;
+          r.postfix = buf;
+          r.size = s;
+          r.op = op;
+          r.rank = best[i];
+          r.status = host_check(r.postfix, hs_[i]) ? SIMBA_OK : SIMBA_E_INTERNAL;
+          r.seconds = now;
+          active[i] = 0;
+        } else if (fl[0]) {
+          r.status = SIMBA_BUDGET;
+          r.seconds = now;
+          active[i] = 0;
+        } else {
+          r.candidates += ct.n[s][8];
+          if (++size[i] > last) {
+            r.status = SIMBA_NOT_FOUND;
+            r.seconds = now;
+            active[i] = 0;
+          }
+        }
+      }
+    }
+    SB_CUDA(cudaEventRecord(e1_, stream_));
+    SB_CUDA(cudaEventSynchronize(e1_));
+    float ms = 0;
+    SB_CUDA(cudaEventElapsedTime(&ms, e0_, e1_));
+    *device_ms = ms;
+    for (auto& r : *outs) *candidates += r.candidates;
+    return 0;
+  }
+
+ private:
+  const ItemTemplate& get_template(const CountTable& ct, int T, int s, uint64_t mask,
+                                   uint64_t unit_target) {
+    int ul = 0;
+    while ((1ULL << ul) < unit_target && ul < 63) ++ul;
+    const uint64_t key =
+        ((uint64_t)ul << 24) | ((uint64_t)ct.terms << 16) | ((uint64_t)T << 8) | (uint64_t)s;
+    auto f = templates_.find(key);
+    if (f != templates_.end()) return f->second;
+    ItemTemplate tp;
+    std::vector<Item> items;
+    if (s <= T) {
+      Item it;
+      memset(&it, 0, sizeof(it));
+      it.bottom = (int8_t)s;
+      it.coefv = 1;
+      it.nv = ct.n[s][8];
+      items.push_back(it);
+    } else if ((s - 1) / 2 > T) {
+      tp.ok = false;
+    } else {
+      Enumerator en;
+      en.ct = &ct;
+      en.T = T;
+      en.mask = mask;
+      en.items = &items;
+      std::vector<Level> lv;
+      std::vector<ChainClass> top{{1, 0, 0}};
+      en.rec(s, lv, 1, 0, top);
+      if (en.too_deep) tp.ok = false;
+    }
+    if (tp.ok) {
+      for (auto& it : items) {
+        for (int l = 0; l < it.depth; ++l)
+          if (it.lv[l].kind == 1) it.lv[l].c &= mask;
+        finish_structure(it, mask);
+      }
+      fuse_small(items, &tp.small, &tp.nctxs, ct, 1ULL << 22);
+      for (auto& it : items) finish_layout(it, kThreads, unit_target);
+      std::stable_sort(items.begin(), items.end(),
+                       [](const Item& a, const Item& b) { return a.base < b.base; });
+      for (auto& it : items) {
+        tp.units += it.cblocks * it.vblocks;
+        tp.cand += (double)it.nctx * (double)it.nv;
+        const double w = sizeof(W) == 8 ? 2.0 : 1.0;
+        double c = it.full ? w : w + 1.0;
+        for (int l = it.inv; l < it.depth; ++l)
+          c += (it.lv[l].kind == 0 && it.lv[l].op == OP_MUL) ? (sizeof(W) == 8 ? 3.0 : 1.0) : w;
+        tp.alg += (double)it.nctx * (double)it.nv * c;
+      }
+      uint64_t ub = 0;
+      for (auto& it : items) {  // unit_begin relative to the list
+        it.unit_begin = ub;
+        ub += it.cblocks * it.vblocks;
+      }
+      TmplDesc td;
+      td.item_off = all_items_.size();
+      td.nitems = (unsigned)items.size();
+      td.small_off = all_small_.size();
+      td.nsmall = (unsigned)tp.small.size();
+      all_items_.insert(all_items_.end(), items.begin(), items.end());
+      all_small_.insert(all_small_.end(), tp.small.begin(), tp.small.end());
+      tp.id = (int)tdescs_.size();
+      tdescs_.push_back(td);
+      tmpl_dirty_ = true;
+      tp.items = std::move(items);
+    }
+    return templates_.emplace(key, std::move(tp)).first->second;
+  }
+
+  std::vector<HostInstance> hs_;
+  EngineOptions o_;
+  int64_t inst_budget_;
+  uint64_t unit_target_;
+  cudaStream_t stream_ = nullptr;
+  bool own_stream_ = true;
+  cudaEvent_t e0_ = nullptr, e1_ = nullptr;
+  std::vector<CountTable> cts_;
+  std::map<uint64_t, ItemTemplate> templates_;
+  std::vector<Item> all_items_, all_small_;  // every spine list, concatenated
+  std::vector<TmplDesc> tdescs_;
+  bool tmpl_dirty_ = false;
+  std::vector<Task> tasks_;
+  std::vector<BuildJob<W>> build_jobs_;
+  DevBuf d_tab_, d_smp_, d_cts_, d_best_, d_desc_, d_scal_, d_items_, d_small_, d_ctx_, d_jobs_,
+      d_tasks_, d_tdesc_;
+};
+
+template <class W>
+int batch_typed(const std::vector<HostInstance>& hs, int max_size, const EngineOptions& o,
+                int64_t inst_table_bytes, BatchOutcome* out) {
+  const uint64_t unit_target = 1ULL << (o.unit_log2 > 0 ? std::min(o.unit_log2, 40) : 22);
+  Batch<W> b(hs, o, inst_table_bytes > 0 ? inst_table_bytes : (8LL << 20), unit_target);
+  std::vector<typename Batch<W>::Out> r;
+  const int rc = b.run(max_size, &r, &out->device_ms, &out->rounds, &out->launches, &out->evaluated,
+                       &out->candidates, &out->alg_ops, &out->kernel_ms);
+  if (rc) return rc;
+  out->items.resize(r.size());
+  for (size_t i = 0; i < r.size(); ++i) {
+    BatchItemOutcome& d = out->items[i];
+    d.status = r[i].status;
+    d.size = r[i].size;
+    d.op = r[i].op;
+    d.rank = r[i].rank;
+    d.postfix = r[i].postfix;
+    d.seconds = r[i].seconds;
+    d.candidates = r[i].candidates;
+  }
+  return 0;
+}
 
 // Creates and initialises a session for word type W (search_u32.cu / search_u64.cu).
 template <class W>

@@ -90,6 +90,7 @@ static int solve_static_typed(const HostInstance& h, int max_size, const EngineO
   // Fixed region: counts | scalars | samples (16-byte padded).
   unsigned char* p_counts = base;
   unsigned long long* p_scal = reinterpret_cast<unsigned long long*>(base + 4096);
+  unsigned char* p_desc = base + 4096 + 256;  // one InstDesc (< 512 bytes)
   unsigned char* p_in = base + 8192;
   const size_t nin16 = ((size_t)h.S * h.k * sizeof(W) + 15) / 16;
   const size_t nout16 = ((size_t)h.S * sizeof(W) + 15) / 16;
@@ -219,22 +220,28 @@ static int solve_static_typed(const HostInstance& h, int max_size, const EngineO
     const unsigned long long init[3] = {0, ~0ULL, 0};
     SB_CUDA(cudaMemcpyAsync(p_scal, init, sizeof(init), cudaMemcpyHostToDevice, st));
     SB_CUDA(cudaMemsetAsync(p_scal + 4, 0, 4 * sizeof(unsigned long long), st));
+    InstDesc<W> d;
+    memset(&d, 0, sizeof(d));
+    for (int t = 1; t <= built; ++t) d.tab[t] = tab(t);
+    d.in = reinterpret_cast<const W*>(p_in);
+    d.out = reinterpret_cast<const W*>(p_out);
+    d.counts = reinterpret_cast<const unsigned long long*>(p_counts);
+    d.best = p_scal + 1;
+    d.target = (W)h.out[0];
+    d.size = s;
+    d.S = h.S;
+    d.K = h.k;
+    SB_CUDA(cudaMemcpyAsync(p_desc, &d, sizeof(d), cudaMemcpyHostToDevice, st));
     Params<W> p;
     memset(&p, 0, sizeof(p));
-    for (int t = 1; t <= built; ++t) p.tab[t] = tab(t);
+    p.insts = reinterpret_cast<const InstDesc<W>*>(p_desc);
     p.items = p_items;
-    p.in = reinterpret_cast<const W*>(p_in);
-    p.out = reinterpret_cast<const W*>(p_out);
-    p.counts = reinterpret_cast<const unsigned long long*>(p_counts);
     p.counter = p_scal + 0;
-    p.best = p_scal + 1;
     p.evaluated = p_scal + 2;
     p.start_ns = p_scal + 3;
     p.flags = reinterpret_cast<int*>(p_scal + 4);
-    p.target = (W)h.out[0];
-    p.size = s;
-    p.S = h.S;
-    p.K = h.k;
+    p.maxS = h.S;
+    p.maxK = h.k;
     p.budget_ns = o.budget_s > 0 ? (unsigned long long)(o.budget_s * 1e9) : 0;
     p.nitems = (int)items.size();
     p.total_units = units;

@@ -8,4 +8,9 @@ int make_search_u32(const HostInstance& h, const EngineOptions& o, SearchSession
   return make_search_typed<uint32_t>(h, o, out);
 }
 
+int batch_u32(const std::vector<HostInstance>& hs, int max_size, const EngineOptions& o,
+              int64_t inst_table_bytes, BatchOutcome* out) {
+  return batch_typed<uint32_t>(hs, max_size, o, inst_table_bytes, out);
+}
+
 }  // namespace simba

@@ -219,6 +219,7 @@ class Instance:
     formula: Optional[str] = None   # postfix of the generating expression
     const_one: bool = False         # last variable is the constant 1
     meta: dict = field(default_factory=dict)
+    unit_log2: int = 0              # batch work-unit size (set by the autotuner)
 
     @property
     def num_examples(self) -> int:

@@ -147,3 +147,31 @@ def test_cli_dropin(tmp_path, oracle, golden):
         assert expr == S.format_postfix(o["postfix"])
     out = subprocess.run([str(exe)], capture_output=True, text=True)
     assert out.returncode == 0 and out.stdout == "" and "maxLen" in out.stderr
+
+
+def test_shards_of_a_size_combine_to_the_full_search(oracle):
+    """Work units split across 3 shards (as over 3 GPUs): the minimum of the
+    shards' best ranks is the single-GPU answer, size by size."""
+    from simba_b200 import dist as D
+    for seed in range(3):
+        inst = make_instance(10, 2, 32, 60 + seed, word_bits=64)
+        full = S.solve(inst, 12)
+        counts = S.count_table(12, inst.num_variables)
+        with S.Session(inst) as ss:
+            res = [D.solve_sharded(ss, 12, shard, 3, lambda x: x, counts) for shard in range(3)]
+        best = min((r["rank"] for r in res if r["found"]), default=None)
+        if full.found:
+            sizes = {r["size"] for r in res if r["found"]}
+            assert min(sizes) == full.size
+            # per size, only shards of the minimal size compete
+            best = min(r["rank"] for r in res if r["found"] and r["size"] == full.size)
+            assert best == full.rank
+        with S.Session(inst) as ss:
+            for size in range(2, 12):
+                parts = [ss.search_size(size, sh, 3) for sh in range(3)]
+                whole = ss.search_size(size, 0, 1)
+                mins = [p["best_rank"] for p in parts if p["best_rank"] is not None]
+                assert (min(mins) if mins else None) == whole["best_rank"]
+                if whole["best_rank"] is not None:
+                    break  # units above a match may be skipped differently
+                assert sum(p["evaluated"] for p in parts) == whole["evaluated"]
