@@ -63,7 +63,13 @@ typedef struct {
                             as written (stores repeated vectors)                */
   int32_t unit_log2;     /* log2 of candidates per work unit, 0 = 22 (autotuned
                             per bucket by the Python autotuner)                  */
-  int32_t reserved[2];
+  const float *class_prior; /* guided search: 64 shape-class priors (see
+                            simba_shape_class).  Sizes are still searched in
+                            order and every candidate of the sizes below the
+                            answer is evaluated; inside a size the spines run
+                            in decreasing prior and the search stops at the
+                            first verified match, which has the minimal size
+                            but need not have the minimum rank.  NULL = plain */
 } simba_options;
 
 typedef struct {
@@ -219,6 +225,35 @@ void simba_instance_free(simba_instance *inst);
  * denominator of the search kernels' roofline (no counterpart in the
  * reference, which reports no roofline). */
 int simba_int_peak(int device, double *lane_ops_per_s);
+
+/* Shape class of an expression (the guided search's unit of priority and
+ * the label the proposal learns): 8 * root operator + min(left operand size,
+ * 7) for a binary root, 8 * root operator + min(length of the unary chain at
+ * the root, 7) for a unary root.  Returns 0..63 or a negative code. */
+int simba_shape_class(const char *postfix);
+
+/* Learned proposal: a 3-layer MLP (8192 -> 512 -> 512 -> 64) over bit-level
+ * features of an instance's samples, predicting the shape class of its
+ * minimal expression; BF16 tensor-core GEMMs with FP32 accumulation,
+ * hand-written backward pass and Adam.  No counterpart in the reference.
+ * Parameters are flattened W1[8192x512], b1[512], W2[512x512], b2[512],
+ * W3[512x64], b3[64] (row-major, input x output). */
+typedef struct simba_mlp simba_mlp;
+int64_t simba_mlp_param_count(void);
+int simba_mlp_create(int device, uint64_t seed, simba_mlp **mlp);
+void simba_mlp_destroy(simba_mlp *mlp);
+/* One Adam step on a minibatch; *loss = mean cross-entropy before the step. */
+int simba_mlp_train_step(simba_mlp *mlp, const simba_instance *insts, int n, const int32_t *labels,
+                         float lr, float *loss);
+/* Gradients of the mean cross-entropy (param_count floats), no update. */
+int simba_mlp_gradients(simba_mlp *mlp, const simba_instance *insts, int n, const int32_t *labels,
+                        float *grads, float *loss);
+/* Class probabilities, n x 64. */
+int simba_mlp_predict(simba_mlp *mlp, const simba_instance *insts, int n, float *probs);
+/* The features the network reads, n x 8192 (values -1, 0, +1). */
+int simba_mlp_features(simba_mlp *mlp, const simba_instance *insts, int n, float *features);
+int simba_mlp_get_params(simba_mlp *mlp, float *params);
+int simba_mlp_set_params(simba_mlp *mlp, const float *params);
 
 const char *simba_version(void);
 const char *simba_status_string(int status);

@@ -43,7 +43,7 @@ class _Options(C.Structure):
                 ("engine", C.c_int32), ("budget_seconds", C.c_double),
                 ("table_bytes", C.c_int64), ("stream", C.c_uint64),
                 ("vfb_cache_rows", C.c_int64), ("vfb_reference_dedup", C.c_int32),
-                ("unit_log2", C.c_int32), ("reserved", C.c_int32 * 2)]
+                ("unit_log2", C.c_int32), ("class_prior", C.POINTER(C.c_float))]
 
 
 class _BatchResult(C.Structure):
@@ -168,7 +168,7 @@ class _Arrays:
 
 def _opts(device=0, complete=False, verbose=False, naive=False, budget=0.0,
           table_bytes=0, stream=0, cache_rows=0, reference_dedup=False,
-          unit_log2=0) -> _Options:
+          unit_log2=0, class_prior=None) -> _Options:
     o = _Options()
     o.device = device
     o.size_range = 1 if complete else 0
@@ -180,6 +180,8 @@ def _opts(device=0, complete=False, verbose=False, naive=False, budget=0.0,
     o.vfb_cache_rows = int(cache_rows)
     o.vfb_reference_dedup = 1 if reference_dedup else 0
     o.unit_log2 = int(unit_log2)
+    if class_prior is not None:  # the caller keeps the array alive for the call
+        o.class_prior = class_prior.ctypes.data_as(C.POINTER(C.c_float))
     return o
 
 

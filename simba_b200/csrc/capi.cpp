@@ -143,6 +143,7 @@ static EngineOptions to_opts(const simba_options* o) {
     e.table_bytes = o->table_bytes;
     e.stream = o->stream;
     e.unit_log2 = o->unit_log2;
+    e.class_prior = o->class_prior;
   }
   return e;
 }
@@ -239,6 +240,23 @@ int read_instance_json(const std::string& path, HostInstance* h) {
 }  // namespace simba
 
 using namespace simba;
+
+struct simba_mlp {
+  Mlp* m = nullptr;
+};
+
+static int to_hosts(const simba_instance* insts, int n, std::vector<HostInstance>* hs) {
+  if (!insts || n < 1) {
+    set_last_error("empty instance list");
+    return SIMBA_E_ARG;
+  }
+  hs->resize(n);
+  for (int i = 0; i < n; ++i) {
+    const int rc = to_host(insts + i, &(*hs)[i]);
+    if (rc) return rc;
+  }
+  return 0;
+}
 
 struct simba_session {
   SearchSession* s = nullptr;
@@ -521,6 +539,98 @@ void simba_instance_free(simba_instance* inst) {
 int simba_int_peak(int device, double* lane_ops_per_s) {
   if (!lane_ops_per_s) return SIMBA_E_ARG;
   return measure_int_peak(device, lane_ops_per_s);
+}
+
+int simba_shape_class(const char* postfix) {
+  if (!postfix) return SIMBA_E_ARG;
+  const int len = (int)strlen(postfix);
+  if (len < 2) return len == 1 ? 0 : SIMBA_E_ARG;
+  const int op = char_op(postfix[len - 1]);
+  if (op < 0) return SIMBA_E_ARG;
+  if (is_unary(op)) {
+    int m = 0;
+    for (int i = len - 1; i >= 0 && char_op(postfix[i]) >= 0 && is_unary(char_op(postfix[i])); --i) ++m;
+    return op * 8 + (m < 7 ? m : 7);
+  }
+  int need = 1, f = -1;
+  for (int i = len - 2; i >= 0; --i) {
+    const int o = char_op(postfix[i]);
+    need -= 1;
+    if (o >= 0) need += is_unary(o) ? 1 : 2;
+    if (need == 0) {
+      f = i;
+      break;
+    }
+  }
+  if (f <= 0) return SIMBA_E_ARG;
+  return op * 8 + (f < 7 ? f : 7);
+}
+
+int64_t simba_mlp_param_count(void) { return (int64_t)mlp_param_count(); }
+
+int simba_mlp_create(int device, uint64_t seed, simba_mlp** mlp) {
+  if (!mlp) return SIMBA_E_ARG;
+  *mlp = nullptr;
+  auto* h = new simba_mlp();
+  const int rc = mlp_create(device, seed, &h->m);
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  *mlp = h;
+  return 0;
+}
+
+void simba_mlp_destroy(simba_mlp* mlp) {
+  if (!mlp) return;
+  mlp_destroy(mlp->m);
+  delete mlp;
+}
+
+int simba_mlp_train_step(simba_mlp* mlp, const simba_instance* insts, int n, const int32_t* labels,
+                         float lr, float* loss) {
+  if (!mlp || !labels) return SIMBA_E_ARG;
+  std::vector<HostInstance> hs;
+  int rc = to_hosts(insts, n, &hs);
+  if (rc) return rc;
+  for (int i = 0; i < n; ++i)
+    if (labels[i] < 0 || labels[i] >= 64) return SIMBA_E_ARG;
+  return mlp_train_step(mlp->m, hs, labels, lr, loss);
+}
+
+int simba_mlp_gradients(simba_mlp* mlp, const simba_instance* insts, int n, const int32_t* labels,
+                        float* grads, float* loss) {
+  if (!mlp || !labels || !grads) return SIMBA_E_ARG;
+  std::vector<HostInstance> hs;
+  int rc = to_hosts(insts, n, &hs);
+  if (rc) return rc;
+  return mlp_gradients(mlp->m, hs, labels, grads, loss);
+}
+
+int simba_mlp_predict(simba_mlp* mlp, const simba_instance* insts, int n, float* probs) {
+  if (!mlp || !probs) return SIMBA_E_ARG;
+  std::vector<HostInstance> hs;
+  int rc = to_hosts(insts, n, &hs);
+  if (rc) return rc;
+  return mlp_predict(mlp->m, hs, probs);
+}
+
+int simba_mlp_features(simba_mlp* mlp, const simba_instance* insts, int n, float* features) {
+  if (!mlp || !features) return SIMBA_E_ARG;
+  std::vector<HostInstance> hs;
+  int rc = to_hosts(insts, n, &hs);
+  if (rc) return rc;
+  return mlp_features(mlp->m, hs, features);
+}
+
+int simba_mlp_get_params(simba_mlp* mlp, float* params) {
+  if (!mlp || !params) return SIMBA_E_ARG;
+  return mlp_get_params(mlp->m, params);
+}
+
+int simba_mlp_set_params(simba_mlp* mlp, const float* params) {
+  if (!mlp || !params) return SIMBA_E_ARG;
+  return mlp_set_params(mlp->m, params);
 }
 
 const char* simba_version(void) { return "simba_b200 0.1 (sm_100a)"; }

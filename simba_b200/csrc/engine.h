@@ -30,6 +30,7 @@ struct EngineOptions {
   int stop_on_match = 1;     // 0: evaluate whole sizes (throughput sweeps)
   uint64_t stream = 0;       // caller's cudaStream_t, 0 = own stream
   int unit_log2 = 0;         // log2 candidates per work unit, 0 = 22
+  const float* class_prior = nullptr;  // guided search: 64 shape-class priors
 };
 
 // Per-solve outcome filled by the engines (capi.cpp formats the strings).
@@ -105,6 +106,19 @@ struct BatchOutcome {
 // (search_impl.cuh: Batch).  inst_table_bytes caps each instance's tables.
 int batch_solve(const std::vector<HostInstance>& hs, int max_size, const EngineOptions& o,
                 int64_t inst_table_bytes, BatchOutcome* out);
+
+// Learned proposal (mlp.cu).
+class Mlp;
+long long mlp_param_count();
+int mlp_create(int device, unsigned long long seed, Mlp** out);
+void mlp_destroy(Mlp* m);
+int mlp_train_step(Mlp* m, const std::vector<HostInstance>& hs, const int* labels, float lr, float* loss);
+int mlp_gradients(Mlp* m, const std::vector<HostInstance>& hs, const int* labels, float* grads,
+                  float* loss);
+int mlp_predict(Mlp* m, const std::vector<HostInstance>& hs, float* probs);
+int mlp_features(Mlp* m, const std::vector<HostInstance>& hs, float* out);
+int mlp_get_params(Mlp* m, float* h);
+int mlp_set_params(Mlp* m, const float* h);
 
 // Read an instance file in the reference JSON schema.
 int read_instance_json(const std::string& path, HostInstance* h);

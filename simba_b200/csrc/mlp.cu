@@ -1,0 +1,463 @@
+// Learned proposal for the guided search: a 3-layer MLP over bit-level
+// features of an instance's samples, predicting the shape class of the
+// minimal expression (root operator x root split / unary-chain length,
+// 8 x 8 = 64 classes).  No counterpart in the reference.
+//
+//   features  X[b] = 8192 values in {-1, 0, +1}: for the first 64 samples
+//             (repeated cyclically when an instance has fewer) 128 features
+//             each: the 64 bits of the output word, then the low 16 bits of
+//             (output XOR variable j) for j = 0..3 (0 when the variable does
+//             not exist).
+//   network   Z1 = X W1 + b1, H1 = relu(Z1), Z2 = H1 W2 + b2, H2 = relu(Z2),
+//             Z3 = H2 W3 + b3, p = softmax(Z3), loss = mean cross-entropy.
+//   GEMMs     BF16 operands, FP32 accumulation, tensor cores through
+//             mma.sync m16n8k16 (64x64 CTA tiles, four warps of 32x32).
+//   training  hand-written backward pass and Adam (FP32 master weights,
+//             BF16 copies feed the GEMMs).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "cuda_util.h"
+#include "engine.h"
+
+namespace simba {
+
+typedef __nv_bfloat16 bf16;
+
+constexpr int kFeat = 8192, kHid = 512, kCls = 64, kFeatSamples = 64, kFeatPerSample = 128;
+
+// ---------------------------------------------------------------- features
+
+struct FeatInst {
+  unsigned long long in_off, out_off;  // word offsets into the packed arrays
+  int S, K;
+};
+
+__global__ void features_kernel(const unsigned long long* in, const unsigned long long* out,
+                                const FeatInst* fi, int n, bf16* X) {
+  const long long total = (long long)n * kFeat;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(g / kFeat), f = (int)(g % kFeat);
+    const FeatInst d = fi[b];
+    const int smp = (f / kFeatPerSample) % d.S;
+    const int j = f % kFeatPerSample;
+    const unsigned long long y = out[d.out_off + smp];
+    float v;
+    if (j < 64) {
+      v = ((y >> j) & 1ULL) ? 1.f : -1.f;
+    } else {
+      const int var = (j - 64) / 16, bit = (j - 64) % 16;
+      if (var < d.K) {
+        const unsigned long long x = in[d.in_off + (unsigned long long)smp * d.K + var];
+        v = (((y ^ x) >> bit) & 1ULL) ? 1.f : -1.f;
+      } else {
+        v = 0.f;
+      }
+    }
+    X[g] = __float2bfloat16(v);
+  }
+}
+
+// ---------------------------------------------------------------- GEMM
+
+// C[M x N] = op(A)[M x K] * op(B)[K x N] (+ bias[n]), FP32 out.
+// op(A)(m,k) = TA ? A[k*lda + m] : A[m*lda + k]
+// op(B)(k,n) = TB ? B[n*ldb + k] : B[k*ldb + n]
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(128) gemm_bf16_kernel(int M, int N, int K, const bf16* A, int lda,
+                                                        const bf16* B, int ldb, float* C, int ldc,
+                                                        const float* bias) {
+  constexpr int BM = 64, BN = 64, BK = 32, PAD = 8;
+  __shared__ __align__(16) bf16 As[BM][BK + PAD];  // m x k
+  __shared__ __align__(16) bf16 Bs[BN][BK + PAD];  // n x k
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  float acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.f;
+  const bf16 zero = __float2bfloat16(0.f);
+  for (int k0 = 0; k0 < K; k0 += BK) {
+    for (int e = tid; e < BM * BK; e += 128) {
+      const int mm = e / BK, kk = e % BK;
+      const int gm = m0 + mm, gk = k0 + kk;
+      bf16 va = zero;
+      if (gm < M && gk < K) va = TA ? A[(long long)gk * lda + gm] : A[(long long)gm * lda + gk];
+      As[mm][kk] = va;
+      const int gn = n0 + mm;
+      bf16 vb = zero;
+      if (gn < N && gk < K) vb = TB ? B[(long long)gn * ldb + gk] : B[(long long)gk * ldb + gn];
+      Bs[mm][kk] = vb;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int ks = 0; ks < BK; ks += 16) {
+      unsigned a[2][4], b[4][2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int r = wm + i * 16 + g;
+        a[i][0] = *reinterpret_cast<const unsigned*>(&As[r][ks + 2 * t]);
+        a[i][1] = *reinterpret_cast<const unsigned*>(&As[r + 8][ks + 2 * t]);
+        a[i][2] = *reinterpret_cast<const unsigned*>(&As[r][ks + 8 + 2 * t]);
+        a[i][3] = *reinterpret_cast<const unsigned*>(&As[r + 8][ks + 8 + 2 * t]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int c = wn + j * 8 + g;
+        b[j][0] = *reinterpret_cast<const unsigned*>(&Bs[c][ks + 2 * t]);
+        b[j][1] = *reinterpret_cast<const unsigned*>(&Bs[c][ks + 8 + 2 * t]);
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          asm volatile(
+              "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+              "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+              : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
+              : "r"(a[i][0]), "r"(a[i][1]), "r"(a[i][2]), "r"(a[i][3]), "r"(b[j][0]), "r"(b[j][1]));
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int row = m0 + wm + i * 16 + g + (r >= 2 ? 8 : 0);
+        const int col = n0 + wn + j * 8 + 2 * t + (r & 1);
+        if (row < M && col < N) C[(long long)row * ldc + col] = acc[i][j][r] + (bias ? bias[col] : 0.f);
+      }
+}
+
+template <bool TA, bool TB>
+static void gemm(cudaStream_t st, int M, int N, int K, const bf16* A, int lda, const bf16* B, int ldb,
+                 float* C, int ldc, const float* bias) {
+  dim3 grid((N + 63) / 64, (M + 63) / 64);
+  gemm_bf16_kernel<TA, TB><<<grid, 128, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc, bias);
+}
+
+// ---------------------------------------------------------------- elementwise
+
+__global__ void relu_bf16_kernel(const float* Z, bf16* H, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    H[i] = __float2bfloat16(fmaxf(Z[i], 0.f));
+}
+
+// dZ = dH * (Z > 0), as BF16 for the next GEMMs
+__global__ void relu_back_kernel(const float* dH, const float* Z, bf16* dZ, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    dZ[i] = __float2bfloat16(Z[i] > 0.f ? dH[i] : 0.f);
+}
+
+// One warp per row: softmax of the 64 logits, probabilities out, and (with
+// labels) the cross-entropy summed into *loss and dZ = (p - onehot) / B.
+__global__ void softmax_ce_kernel(const float* Z, const int* labels, int B, float* P, bf16* dZ,
+                                  float* loss) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= B) return;
+  const float* z = Z + (long long)warp * kCls;
+  float a = z[lane], b = z[lane + 32];
+  float mx = fmaxf(a, b);
+  for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  float ea = expf(a - mx), eb = expf(b - mx);
+  float s = ea + eb;
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  const float pa = ea / s, pb = eb / s;
+  if (P) {
+    P[(long long)warp * kCls + lane] = pa;
+    P[(long long)warp * kCls + lane + 32] = pb;
+  }
+  if (labels) {
+    const int y = labels[warp];
+    if (lane == (y & 31)) {
+      const float py = y < 32 ? pa : pb;
+      atomicAdd(loss, -logf(fmaxf(py, 1e-30f)));
+    }
+    const float inv = 1.f / (float)B;
+    dZ[(long long)warp * kCls + lane] = __float2bfloat16((pa - (lane == y ? 1.f : 0.f)) * inv);
+    dZ[(long long)warp * kCls + lane + 32] = __float2bfloat16((pb - (lane + 32 == y ? 1.f : 0.f)) * inv);
+  }
+}
+
+// column sums of a B x N BF16 matrix into FP32 (bias gradients)
+__global__ void colsum_kernel(const bf16* D, int B, int N, float* out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  float s = 0.f;
+  for (int r = 0; r < B; ++r) s += __bfloat162float(D[(long long)r * N + c]);
+  out[c] = s;
+}
+
+// Adam (Kingma & Ba 2015) on FP32 master weights; refreshes the BF16 copy.
+__global__ void adam_kernel(float* w, const float* g, float* m, float* v, bf16* wb, long long n,
+                            float lr, float b1, float b2, float eps, float c1, float c2) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    w[i] = wi;
+    if (wb) wb[i] = __float2bfloat16(wi);
+  }
+}
+
+__global__ void to_bf16_kernel(const float* a, bf16* b, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    b[i] = __float2bfloat16(a[i]);
+}
+
+// ---------------------------------------------------------------- model
+
+static const long long kSizes[6] = {(long long)kFeat * kHid, kHid, (long long)kHid * kHid, kHid,
+                                    (long long)kHid * kCls, kCls};
+
+long long mlp_param_count() {
+  long long s = 0;
+  for (long long x : kSizes) s += x;
+  return s;
+}
+
+class Mlp {
+ public:
+  explicit Mlp(int device) : dev_(device) {}
+  ~Mlp() {
+    if (st_) cudaStreamDestroy(st_);
+  }
+
+  int init(unsigned long long seed) {
+    SB_CUDA(cudaSetDevice(dev_));
+    SB_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    const long long P = mlp_param_count();
+    SB_CUDA(w_.reserve(P * 4));
+    SB_CUDA(g_.reserve(P * 4));
+    SB_CUDA(m_.reserve(P * 4));
+    SB_CUDA(v_.reserve(P * 4));
+    SB_CUDA(wb_.reserve(P * 2));
+    SB_CUDA(loss_.reserve(16));
+    // He-uniform initialisation of the weights, zero biases
+    std::vector<float> h(P, 0.f);
+    std::mt19937_64 rng(seed);
+    long long off = 0;
+    const int fan_in[3] = {kFeat, kHid, kHid};
+    for (int l = 0; l < 3; ++l) {
+      const float lim = std::sqrt(6.f / (float)fan_in[l]);
+      std::uniform_real_distribution<float> U(-lim, lim);
+      for (long long i = 0; i < kSizes[2 * l]; ++i) h[off + i] = U(rng);
+      off += kSizes[2 * l] + kSizes[2 * l + 1];
+    }
+    return set_params(h.data());
+  }
+
+  int set_params(const float* h) {
+    const long long P = mlp_param_count();
+    SB_CUDA(cudaMemcpy(w_.p, h, P * 4, cudaMemcpyHostToDevice));
+    SB_CUDA(cudaMemset(m_.p, 0, P * 4));
+    SB_CUDA(cudaMemset(v_.p, 0, P * 4));
+    to_bf16_kernel<<<1024, 256, 0, st_>>>(w_.as<float>(), wb_.as<bf16>(), P);
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaStreamSynchronize(st_));
+    step_ = 0;
+    return 0;
+  }
+
+  int get_params(float* h) {
+    SB_CUDA(cudaMemcpy(h, w_.p, mlp_param_count() * 4, cudaMemcpyDeviceToHost));
+    return 0;
+  }
+
+  // Features of n instances into Xd (device, n x 8192 BF16).
+  int features(const std::vector<HostInstance>& hs, DevBuf* Xd) {
+    const int n = (int)hs.size();
+    std::vector<unsigned long long> in, out;
+    std::vector<FeatInst> fi(n);
+    for (int i = 0; i < n; ++i) {
+      fi[i].in_off = in.size();
+      fi[i].out_off = out.size();
+      fi[i].S = hs[i].S;
+      fi[i].K = hs[i].k;
+      in.insert(in.end(), hs[i].in.begin(), hs[i].in.end());
+      out.insert(out.end(), hs[i].out.begin(), hs[i].out.end());
+    }
+    SB_CUDA(fin_.reserve(std::max<size_t>(1, in.size()) * 8));
+    SB_CUDA(fout_.reserve(std::max<size_t>(1, out.size()) * 8));
+    SB_CUDA(finst_.reserve(std::max(1, n) * sizeof(FeatInst)));
+    SB_CUDA(Xd->reserve((size_t)std::max(1, n) * kFeat * 2));
+    SB_CUDA(cudaMemcpyAsync(fin_.p, in.data(), in.size() * 8, cudaMemcpyHostToDevice, st_));
+    SB_CUDA(cudaMemcpyAsync(fout_.p, out.data(), out.size() * 8, cudaMemcpyHostToDevice, st_));
+    SB_CUDA(cudaMemcpyAsync(finst_.p, fi.data(), n * sizeof(FeatInst), cudaMemcpyHostToDevice, st_));
+    features_kernel<<<1024, 256, 0, st_>>>(fin_.as<unsigned long long>(), fout_.as<unsigned long long>(),
+                                           finst_.as<FeatInst>(), n, Xd->as<bf16>());
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaStreamSynchronize(st_));
+    return 0;
+  }
+
+  // Forward (and with labels backward) for a batch already featurised in X_.
+  int forward_backward(int B, const int* labels_host, bool backward, float* loss_out, float* probs) {
+    SB_CUDA(z1_.reserve((size_t)B * kHid * 4));
+    SB_CUDA(z2_.reserve((size_t)B * kHid * 4));
+    SB_CUDA(z3_.reserve((size_t)B * kCls * 4));
+    SB_CUDA(h1_.reserve((size_t)B * kHid * 2));
+    SB_CUDA(h2_.reserve((size_t)B * kHid * 2));
+    SB_CUDA(p_.reserve((size_t)B * kCls * 4));
+    SB_CUDA(lab_.reserve((size_t)std::max(1, B) * 4));
+    const bf16* W1 = wb_.as<bf16>();
+    const bf16* W2 = W1 + kSizes[0] + kSizes[1];
+    const bf16* W3 = W2 + kSizes[2] + kSizes[3];
+    const float* b1 = w_.as<float>() + kSizes[0];
+    const float* b2 = b1 + kSizes[1] + kSizes[2];
+    const float* b3 = b2 + kSizes[3] + kSizes[4];
+    const bf16* X = X_.as<bf16>();
+    gemm<false, false>(st_, B, kHid, kFeat, X, kFeat, W1, kHid, z1_.as<float>(), kHid, b1);
+    relu_bf16_kernel<<<512, 256, 0, st_>>>(z1_.as<float>(), h1_.as<bf16>(), (long long)B * kHid);
+    gemm<false, false>(st_, B, kHid, kHid, h1_.as<bf16>(), kHid, W2, kHid, z2_.as<float>(), kHid, b2);
+    relu_bf16_kernel<<<512, 256, 0, st_>>>(z2_.as<float>(), h2_.as<bf16>(), (long long)B * kHid);
+    gemm<false, false>(st_, B, kCls, kHid, h2_.as<bf16>(), kHid, W3, kCls, z3_.as<float>(), kCls, b3);
+    SB_CUDA(cudaMemsetAsync(loss_.p, 0, 4, st_));
+    int* lab = nullptr;
+    if (labels_host) {
+      SB_CUDA(cudaMemcpyAsync(lab_.p, labels_host, B * 4, cudaMemcpyHostToDevice, st_));
+      lab = lab_.as<int>();
+      SB_CUDA(dz3_.reserve((size_t)B * kCls * 2));
+    }
+    softmax_ce_kernel<<<(B * 32 + 255) / 256, 256, 0, st_>>>(z3_.as<float>(), lab, B, p_.as<float>(),
+                                                            lab ? dz3_.as<bf16>() : nullptr,
+                                                            loss_.as<float>());
+    SB_CUDA(cudaGetLastError());
+    if (backward && lab) {
+      SB_CUDA(dh_.reserve((size_t)B * kHid * 4));
+      SB_CUDA(dz2_.reserve((size_t)B * kHid * 2));
+      SB_CUDA(dz1_.reserve((size_t)B * kHid * 2));
+      float* G = g_.as<float>();
+      float* gW1 = G;
+      float* gb1 = gW1 + kSizes[0];
+      float* gW2 = gb1 + kSizes[1];
+      float* gb2 = gW2 + kSizes[2];
+      float* gW3 = gb2 + kSizes[3];
+      float* gb3 = gW3 + kSizes[4];
+      // layer 3
+      gemm<true, false>(st_, kHid, kCls, B, h2_.as<bf16>(), kHid, dz3_.as<bf16>(), kCls, gW3, kCls, nullptr);
+      colsum_kernel<<<1, kCls, 0, st_>>>(dz3_.as<bf16>(), B, kCls, gb3);
+      gemm<false, true>(st_, B, kHid, kCls, dz3_.as<bf16>(), kCls, W3, kCls, dh_.as<float>(), kHid, nullptr);
+      relu_back_kernel<<<512, 256, 0, st_>>>(dh_.as<float>(), z2_.as<float>(), dz2_.as<bf16>(),
+                                             (long long)B * kHid);
+      // layer 2
+      gemm<true, false>(st_, kHid, kHid, B, h1_.as<bf16>(), kHid, dz2_.as<bf16>(), kHid, gW2, kHid, nullptr);
+      colsum_kernel<<<(kHid + 255) / 256, 256, 0, st_>>>(dz2_.as<bf16>(), B, kHid, gb2);
+      gemm<false, true>(st_, B, kHid, kHid, dz2_.as<bf16>(), kHid, W2, kHid, dh_.as<float>(), kHid, nullptr);
+      relu_back_kernel<<<512, 256, 0, st_>>>(dh_.as<float>(), z1_.as<float>(), dz1_.as<bf16>(),
+                                             (long long)B * kHid);
+      // layer 1
+      gemm<true, false>(st_, kFeat, kHid, B, X, kFeat, dz1_.as<bf16>(), kHid, gW1, kHid, nullptr);
+      colsum_kernel<<<(kHid + 255) / 256, 256, 0, st_>>>(dz1_.as<bf16>(), B, kHid, gb1);
+      SB_CUDA(cudaGetLastError());
+    }
+    SB_CUDA(cudaStreamSynchronize(st_));
+    if (loss_out) {
+      float l = 0;
+      SB_CUDA(cudaMemcpy(&l, loss_.p, 4, cudaMemcpyDeviceToHost));
+      *loss_out = l / (float)std::max(1, B);
+    }
+    if (probs) SB_CUDA(cudaMemcpy(probs, p_.p, (size_t)B * kCls * 4, cudaMemcpyDeviceToHost));
+    return 0;
+  }
+
+  int train_step(const std::vector<HostInstance>& hs, const int* labels, float lr, float* loss) {
+    int rc = features(hs, &X_);
+    if (rc) return rc;
+    rc = forward_backward((int)hs.size(), labels, true, loss, nullptr);
+    if (rc) return rc;
+    ++step_;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, (float)step_), c2 = 1.f - std::pow(b2, (float)step_);
+    // biases have no BF16 copy in use; refreshing the whole copy keeps one kernel
+    adam_kernel<<<2048, 256, 0, st_>>>(w_.as<float>(), g_.as<float>(), m_.as<float>(), v_.as<float>(),
+                                       wb_.as<bf16>(), mlp_param_count(), lr, b1, b2, 1e-8f, c1, c2);
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaStreamSynchronize(st_));
+    return 0;
+  }
+
+  int gradients(const std::vector<HostInstance>& hs, const int* labels, float* grads, float* loss) {
+    int rc = features(hs, &X_);
+    if (rc) return rc;
+    rc = forward_backward((int)hs.size(), labels, true, loss, nullptr);
+    if (rc) return rc;
+    SB_CUDA(cudaMemcpy(grads, g_.p, mlp_param_count() * 4, cudaMemcpyDeviceToHost));
+    return 0;
+  }
+
+  int predict(const std::vector<HostInstance>& hs, float* probs) {
+    int rc = features(hs, &X_);
+    if (rc) return rc;
+    return forward_backward((int)hs.size(), nullptr, false, nullptr, probs);
+  }
+
+  int features_host(const std::vector<HostInstance>& hs, float* out) {
+    int rc = features(hs, &X_);
+    if (rc) return rc;
+    std::vector<bf16> tmp((size_t)hs.size() * kFeat);
+    SB_CUDA(cudaMemcpy(tmp.data(), X_.p, tmp.size() * 2, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < tmp.size(); ++i) out[i] = __bfloat162float(tmp[i]);
+    return 0;
+  }
+
+ private:
+  int dev_;
+  cudaStream_t st_ = nullptr;
+  long long step_ = 0;
+  DevBuf w_, g_, m_, v_, wb_, loss_, fin_, fout_, finst_, X_, z1_, z2_, z3_, h1_, h2_, p_, lab_, dz3_, dh_,
+      dz2_, dz1_;
+};
+
+int mlp_create(int device, unsigned long long seed, Mlp** out) {
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= device || device < 0) {
+    cudaGetLastError();
+    set_last_error("no usable CUDA device");
+    return SIMBA_E_NODEV;
+  }
+  Mlp* m = new Mlp(device);
+  const int rc = m->init(seed);
+  if (rc) {
+    delete m;
+    return rc;
+  }
+  *out = m;
+  return 0;
+}
+void mlp_destroy(Mlp* m) { delete m; }
+int mlp_train_step(Mlp* m, const std::vector<HostInstance>& hs, const int* labels, float lr, float* loss) {
+  return m->train_step(hs, labels, lr, loss);
+}
+int mlp_gradients(Mlp* m, const std::vector<HostInstance>& hs, const int* labels, float* grads,
+                  float* loss) {
+  return m->gradients(hs, labels, grads, loss);
+}
+int mlp_predict(Mlp* m, const std::vector<HostInstance>& hs, float* probs) { return m->predict(hs, probs); }
+int mlp_features(Mlp* m, const std::vector<HostInstance>& hs, float* out) { return m->features_host(hs, out); }
+int mlp_get_params(Mlp* m, float* h) { return m->get_params(h); }
+int mlp_set_params(Mlp* m, const float* h) { return m->set_params(h); }
+
+}  // namespace simba

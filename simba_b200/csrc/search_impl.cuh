@@ -85,7 +85,8 @@ struct Level {
   int8_t small_left; // small operand is the left one
   int8_t ts;         // small side size
   int8_t eps;        // chain sign
-  int8_t pad[3];
+  int8_t chain_len;  // chain: number of unary operators it stands for
+  int8_t pad[2];
 };
 
 struct alignas(16) Item {
@@ -104,7 +105,7 @@ struct alignas(16) Item {
   int8_t pad[2];
   uint64_t ctx_off;     // fused: first context in Params::ctxs
   uint32_t inst;        // instance (index into Params::insts)
-  uint32_t pad2;
+  float prio;           // guided search: prior of the spine's shape class
   Level lv[kMaxDepth];
 };
 
@@ -723,7 +724,9 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
         sm.unit_local = local - p.items[ilo].unit_begin;
         const Item& nx = p.items[ilo];
         if (inst < 0) inst = (int)nx.inst;
-        sm.skip = p.stop_on_match && nx.base > *(volatile unsigned long long*)p.insts[inst].best;
+        const unsigned long long cur = *(volatile unsigned long long*)p.insts[inst].best;
+        // 1: minimum rank (skip spines above the best match); 2: any match
+        sm.skip = p.stop_on_match == 1 ? nx.base > cur : (p.stop_on_match == 2 && cur != ~0ULL);
       }
     }
     __syncthreads();
@@ -872,6 +875,8 @@ struct Enumerator {
 
   uint64_t N(int s) const { return ct->n[s][8]; }
 
+  int chain_start = 0;  // size where the current unary chain began
+
   void emit(int size, std::vector<Level>& lv, uint64_t mult, uint64_t base, const ChainClass& k) {
     if (lv.size() + (k.eps == 1 && k.c == 0 ? 0 : 1) > (size_t)kMaxDepth) {
       too_deep = true;
@@ -888,6 +893,7 @@ struct Enumerator {
       L.eps = (int8_t)k.eps;
       L.c = (uint64_t)k.c & mask;
       L.nsmall = 1;
+      L.chain_len = (int8_t)(chain_start - size);
       it.lv[d++] = L;
     }
     it.depth = (int8_t)d;
@@ -927,6 +933,7 @@ struct Enumerator {
       add(-k.eps, k.c, k.off + off_neg * mult);
     }
     rec(size - 1, lv, mult, base, ncls);
+    const int my_chain_start = chain_start;
     // Binary blocks in rank order.
     const int sub = size - 1;
     for (int op = 0; op < 8; ++op) {
@@ -944,6 +951,7 @@ struct Enumerator {
             C.eps = (int8_t)k.eps;
             C.c = (uint64_t)k.c & mask;
             C.nsmall = 1;
+            C.chain_len = (int8_t)(my_chain_start - size);
             lv2.push_back(C);
           }
           Level B;
@@ -972,7 +980,9 @@ struct Enumerator {
             return;
           }
           std::vector<ChainClass> id{{1, 0, 0}};
+          chain_start = big;
           rec(big, lv2, nmult, base + k.off + boff * mult, id);
+          chain_start = my_chain_start;
         }
         boff += N(i) * N(j);
       }
@@ -1035,13 +1045,40 @@ static inline void finish_item(Item& it, int threads, uint64_t mask) {
   finish_layout(it, threads);
 }
 
+// Shape class of a spine (the guided search's unit of priority): root
+// operator x (left operand size, or length of the root's unary chain),
+// capped at 7 -- 64 classes.  A unary chain class merges chains that start
+// with ~ and with neg, so both root operators are returned.
+static inline void spine_classes(const Item& it, int size, int* c0, int* c1) {
+  *c0 = *c1 = -1;
+  if (it.depth == 0) return;
+  const Level& L = it.lv[0];
+  if (L.kind == 1) {
+    const int m = std::min<int>(std::max<int>(L.chain_len, 1), 7);
+    *c0 = OP_NOT * 8 + m;
+    *c1 = OP_NEG * 8 + m;
+    return;
+  }
+  const int left = L.small_left ? L.ts : size - 1 - L.ts;
+  *c0 = L.op * 8 + std::min(left, 7);
+}
+
+static inline float spine_prio(const Item& it, int size, const float* prior) {
+  int a, b;
+  spine_classes(it, size, &a, &b);
+  if (a < 0) return 1e30f;  // a whole tabled size: one spine
+  float p = prior[a];
+  if (b >= 0) p = std::max(p, prior[b]);
+  return p;
+}
+
 // Fully inverted spines with fewer contexts than one work unit holds would
 // each stream their bottom table once; spines sharing a bottom size (and
 // mask kind) are fused into one context list instead, materialised on the
 // device.  Returns the fused work items; `small` receives the member spines
 // with their offsets into the list.
 static inline void fuse_small(std::vector<Item>& items, std::vector<Item>* small, uint64_t* nctxs,
-                              const CountTable& ct, uint64_t max_ctxs) {
+                              const CountTable& ct, uint64_t max_ctxs, bool by_prio = false) {
   std::vector<Item> keep;
   std::vector<Item> groups;
   std::vector<std::vector<size_t>> members;
@@ -1054,12 +1091,15 @@ static inline void fuse_small(std::vector<Item>& items, std::vector<Item>* small
     }
     size_t gi = 0;
     for (; gi < groups.size(); ++gi)
-      if (groups[gi].bottom == it.bottom && groups[gi].full == it.full) break;
+      if (groups[gi].bottom == it.bottom && groups[gi].full == it.full &&
+          (!by_prio || groups[gi].prio == it.prio))
+        break;
     if (gi == groups.size()) {
       Item g;
       memset(&g, 0, sizeof(g));
       g.bottom = it.bottom;
       g.full = it.full;
+      g.prio = it.prio;
       g.fused = 1;
       g.nv = ct.n[(int)it.bottom][8];
       g.base = ~0ULL;
@@ -1325,13 +1365,21 @@ class Search final : public SearchSession {
           if (it.lv[l].kind == 1) it.lv[l].c &= mask_;
         finish_structure(it, mask_);
       }
+      const bool guided = o_.class_prior != nullptr;
+      if (guided)
+        for (auto& it : items) it.prio = spine_prio(it, s, o_.class_prior);
       std::vector<Item> small;
       uint64_t nctxs = 0;
-      fuse_small(items, &small, &nctxs, ct_, 1ULL << 22);
+      fuse_small(items, &small, &nctxs, ct_, 1ULL << 22, guided);
       const uint64_t unit_target = 1ULL << (o_.unit_log2 > 0 ? std::min(o_.unit_log2, 40) : 22);
       for (auto& it : items) finish_layout(it, kThreads, unit_target);
-      std::stable_sort(items.begin(), items.end(),
-                       [](const Item& a, const Item& b) { return a.base < b.base; });
+      if (guided)  // most likely shape classes first; ties in rank order
+        std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) {
+          return a.prio != b.prio ? a.prio > b.prio : a.base < b.base;
+        });
+      else
+        std::stable_sort(items.begin(), items.end(),
+                         [](const Item& a, const Item& b) { return a.base < b.base; });
       uint64_t units = 0;
       for (auto& it : items) {
         it.unit_begin = units;
@@ -1347,7 +1395,7 @@ class Search final : public SearchSession {
       p.total_units = units;
       p.unit_offset = (unsigned long long)shard;
       p.unit_stride = (unsigned long long)nshards;
-      p.stop_on_match = stop ? 1 : 0;
+      p.stop_on_match = stop ? (guided ? 2 : 1) : 0;
       SB_CUDA(cudaEventRecord(evk_, stream_));
       if (nctxs) {
         SB_CUDA(d_small_.reserve(small.size() * sizeof(Item)));

@@ -1,0 +1,171 @@
+"""Learned proposal and guided search.
+
+The proposal is the MLP of the C ABI (``simba_mlp_*``): it reads bit-level
+features of an instance's samples and predicts a prior over the 64 shape
+classes of the minimal expression (root operator x left-operand size or
+root unary-chain length).  The guided search takes that prior: sizes are
+still searched in increasing order and every smaller size is exhausted, so
+the answer has the minimal size; inside a size the spines run in decreasing
+prior and the search stops at the first verified match.  Nothing is pruned:
+with a uniform prior the guided search degenerates to the plain order.
+
+Training data comes from the plain search itself: instances are solved by
+:func:`simba_b200.solve_batch` and labelled with the shape class of their
+answer (:func:`shape_class`).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Iterable, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import (OK, Result, SimbaError, _Arrays, _check, _Instance, lib, solve,
+               solve_batch)
+from .instances import Instance, iter_batch
+
+N_CLASSES = 64
+N_FEATURES = 8192
+
+
+def shape_class(postfix: str) -> int:
+    c = lib().simba_shape_class(postfix.encode())
+    if c < 0:
+        raise SimbaError(f"not an expression: {postfix!r}")
+    return c
+
+
+def _bind():
+    L = lib()
+    if getattr(L, "_mlp_bound", False):
+        return L
+    P = C.POINTER
+    L.simba_shape_class.argtypes = [C.c_char_p]
+    L.simba_mlp_param_count.restype = C.c_int64
+    L.simba_mlp_create.argtypes = [C.c_int, C.c_uint64, P(C.c_void_p)]
+    L.simba_mlp_destroy.argtypes = [C.c_void_p]
+    L.simba_mlp_destroy.restype = None
+    L.simba_mlp_train_step.argtypes = [C.c_void_p, P(_Instance), C.c_int, P(C.c_int32), C.c_float,
+                                       P(C.c_float)]
+    L.simba_mlp_gradients.argtypes = [C.c_void_p, P(_Instance), C.c_int, P(C.c_int32),
+                                      P(C.c_float), P(C.c_float)]
+    L.simba_mlp_predict.argtypes = [C.c_void_p, P(_Instance), C.c_int, P(C.c_float)]
+    L.simba_mlp_features.argtypes = [C.c_void_p, P(_Instance), C.c_int, P(C.c_float)]
+    L.simba_mlp_get_params.argtypes = [C.c_void_p, P(C.c_float)]
+    L.simba_mlp_set_params.argtypes = [C.c_void_p, P(C.c_float)]
+    L._mlp_bound = True
+    return L
+
+
+def _carr(insts: Sequence[Instance]):
+    arrs = [_Arrays(i) for i in insts]
+    return arrs, (_Instance * len(arrs))(*[a.c for a in arrs])
+
+
+def _f32p(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Proposal:
+    """The MLP proposal on one GPU."""
+
+    def __init__(self, device: int = 0, seed: int = 0):
+        L = _bind()
+        self._h = C.c_void_p()
+        _check(L.simba_mlp_create(device, seed, C.byref(self._h)))
+        self.n_params = int(L.simba_mlp_param_count())
+
+    def close(self):
+        if self._h:
+            lib().simba_mlp_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def train_step(self, insts: Sequence[Instance], labels: Sequence[int], lr: float = 1e-3) -> float:
+        arrs, ca = _carr(insts)
+        lab = np.ascontiguousarray(labels, dtype=np.int32)
+        loss = C.c_float()
+        _check(lib().simba_mlp_train_step(self._h, ca, len(insts),
+                                          lab.ctypes.data_as(C.POINTER(C.c_int32)), lr,
+                                          C.byref(loss)))
+        return float(loss.value)
+
+    def gradients(self, insts, labels) -> Tuple[np.ndarray, float]:
+        arrs, ca = _carr(insts)
+        lab = np.ascontiguousarray(labels, dtype=np.int32)
+        g = np.zeros(self.n_params, dtype=np.float32)
+        loss = C.c_float()
+        _check(lib().simba_mlp_gradients(self._h, ca, len(insts),
+                                         lab.ctypes.data_as(C.POINTER(C.c_int32)), _f32p(g),
+                                         C.byref(loss)))
+        return g, float(loss.value)
+
+    def predict(self, insts: Sequence[Instance]) -> np.ndarray:
+        arrs, ca = _carr(insts)
+        p = np.zeros((len(insts), N_CLASSES), dtype=np.float32)
+        _check(lib().simba_mlp_predict(self._h, ca, len(insts), _f32p(p)))
+        return p
+
+    def features(self, insts: Sequence[Instance]) -> np.ndarray:
+        arrs, ca = _carr(insts)
+        x = np.zeros((len(insts), N_FEATURES), dtype=np.float32)
+        _check(lib().simba_mlp_features(self._h, ca, len(insts), _f32p(x)))
+        return x
+
+    def get_params(self) -> np.ndarray:
+        w = np.zeros(self.n_params, dtype=np.float32)
+        _check(lib().simba_mlp_get_params(self._h, _f32p(w)))
+        return w
+
+    def set_params(self, w: np.ndarray) -> None:
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        if w.size != self.n_params:
+            raise ValueError("wrong parameter count")
+        _check(lib().simba_mlp_set_params(self._h, _f32p(w)))
+
+    def save(self, path) -> None:
+        np.save(path, self.get_params())
+
+    def load(self, path) -> None:
+        self.set_params(np.load(path))
+
+
+def label_instances(insts: Sequence[Instance], max_size: int, budget: float = 0.0,
+                    **kw) -> Tuple[List[Instance], np.ndarray]:
+    """Solve with the plain batch search; keep the solved ones with labels."""
+    res, _ = solve_batch(insts, max_size, budget=budget, **kw)
+    keep, labels = [], []
+    for inst, r in zip(insts, res):
+        if r.status == OK:
+            keep.append(inst)
+            labels.append(shape_class(r.postfix))
+    return keep, np.asarray(labels, dtype=np.int32)
+
+
+def train(prop: Proposal, insts: Sequence[Instance], labels: np.ndarray, epochs: int = 3,
+          batch: int = 256, lr: float = 1e-3, seed: int = 0) -> List[float]:
+    """Minibatch Adam over (instances, labels); returns the loss per step."""
+    rng = np.random.default_rng(seed)
+    losses = []
+    n = len(insts)
+    for _ in range(epochs):
+        order = rng.permutation(n)
+        for s in range(0, n, batch):
+            idx = order[s:s + batch]
+            if len(idx) == 0:
+                continue
+            losses.append(prop.train_step([insts[i] for i in idx], labels[idx], lr))
+    return losses
+
+
+def solve_guided(inst: Instance, max_size: int, prior: np.ndarray, **kw) -> Result:
+    """Guided plain search of one instance with a 64-class prior."""
+    pr = np.ascontiguousarray(prior, dtype=np.float32)
+    if pr.size != N_CLASSES:
+        raise ValueError("prior must have 64 entries")
+    return solve(inst, max_size, class_prior=pr, **kw)

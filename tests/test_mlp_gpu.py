@@ -1,0 +1,106 @@
+"""Learned proposal on the GPU: features and gradients against the numpy
+oracle, training, guided search correctness and what the network gains."""
+import numpy as np
+import pytest
+
+from oracle import mlp_ref as R
+import simba_b200 as S
+from simba_b200 import guided as G
+from simba_b200.instances import iter_batch, make_instance
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def prop():
+    p = G.Proposal(seed=1)
+    yield p
+    p.close()
+
+
+def test_features_match_reference(prop):
+    insts = [make_instance(6 + i, 1 + i % 4, (16, 32, 64, 128)[i % 4], 40 + i, word_bits=64)
+             for i in range(6)]
+    X = prop.features(insts)
+    for i, inst in enumerate(insts):
+        assert (X[i] == R.features(inst.inputs, inst.outputs)).all()
+
+
+def test_gradients_match_reference(prop):
+    rng = np.random.default_rng(5)
+    insts = [make_instance(5 + i % 6, 1 + i % 3, 32, 900 + i, word_bits=64) for i in range(24)]
+    labels = rng.integers(0, 64, len(insts)).astype(np.int32)
+    w = prop.get_params()
+    g, loss = prop.gradients(insts, labels)
+    X = np.stack([R.features(i.inputs, i.outputs) for i in insts])
+    rloss, rg, _ = R.forward_backward(w, X, labels)
+    assert abs(loss - rloss) < 1e-3 * max(1.0, abs(rloss))
+    # BF16 operands, FP32 accumulation in a different order: relative error
+    err = np.linalg.norm(g - rg) / np.linalg.norm(rg)
+    assert err < 2e-2, err
+    # per layer too
+    sizes = [8192 * 512, 512, 512 * 512, 512, 512 * 64, 64]
+    o = 0
+    for n in sizes:
+        a, b = g[o:o + n], rg[o:o + n]
+        if np.linalg.norm(b) > 1e-6:
+            assert np.linalg.norm(a - b) / np.linalg.norm(b) < 5e-2
+        o += n
+
+
+def test_training_reduces_loss():
+    p = G.Proposal(seed=2)
+    insts = list(iter_batch(256, 123, sizes=range(3, 9), vars_=(1, 2, 3), samples=(32, 64),
+                            word_bits=64))
+    keep, labels = G.label_instances(insts, 10)
+    assert len(keep) > 200
+    losses = G.train(p, keep, labels, epochs=20, batch=64, lr=1e-3)
+    assert np.mean(losses[-4:]) < 0.7 * np.mean(losses[:4])
+    probs = p.predict(keep[:10])
+    assert probs.shape == (10, 64) and np.allclose(probs.sum(axis=1), 1.0, atol=1e-4)
+    p.close()
+
+
+def test_guided_search_returns_minimal_size(oracle, prop):
+    rng = np.random.default_rng(3)
+    for seed in range(8):
+        inst = make_instance(9, 2, 32, 1300 + seed, word_bits=64)
+        plain = S.solve(inst, 12)
+        prior = rng.random(64).astype(np.float32)
+        g = G.solve_guided(inst, 12, prior)
+        assert g.found == plain.found
+        if plain.found:
+            assert g.size == plain.size
+            assert oracle.check(g.postfix, inst.inputs, inst.outputs, 64)
+            # the sizes below the answer are exhausted in both searches
+            assert g.per_size[:g.size] == plain.per_size[:plain.size]
+
+
+def test_trained_proposal_beats_uniform_order():
+    """What the network gains: candidates evaluated until the first match,
+    trained prior vs uniform prior (= the plain order with any-match stop)."""
+    p = G.Proposal(seed=4)
+    train_insts = list(iter_batch(3000, 10 ** 6, sizes=range(3, 12), vars_=(1, 2, 3),
+                                  samples=(64,), word_bits=64))
+    keep, labels = G.label_instances(train_insts, 11)
+    G.train(p, keep, labels, epochs=4, batch=256, lr=1e-3)
+    test_insts = list(iter_batch(300, 2 * 10 ** 6, sizes=range(9, 13), vars_=(2, 3),
+                                 samples=(64,), word_bits=64))
+    test_keep, test_labels = G.label_instances(test_insts, 12)
+    probs = p.predict(test_keep)
+    acc = float((probs.argmax(axis=1) == test_labels).mean())
+    uniform = np.full(64, 1.0 / 64, dtype=np.float32)
+    ratios = []
+    # small tables and small work units: the final size runs as many spines
+    # in many waves, so the order inside the size decides the work done
+    kw = dict(table_bytes=1 << 20, unit_log2=16)
+    for inst, pr in zip(test_keep, probs):
+        a = G.solve_guided(inst, 12, pr, **kw)
+        b = G.solve_guided(inst, 12, uniform, **kw)
+        assert a.size == b.size
+        if b.evaluated > 10 ** 7:  # only searches long enough for order to matter
+            ratios.append(a.evaluated / b.evaluated)
+    assert len(ratios) >= 10
+    assert acc > 1.5 / 64  # better than chance
+    assert np.median(ratios) < 1.0, (np.median(ratios), acc)
+    p.close()
