@@ -214,12 +214,14 @@ def run_ours(a, rank: int, world: int, local_rank: int) -> None:
         kernel_s = kernel_ms / 1e3
         achieved = alg_ops / kernel_s if kernel_s > 0 else 0.0
         traffic = None
-        prof = ROOT / "profiles" / "spine_kernel_traffic.json"
+        prof = ROOT / "profiles" / "spine_kernel_size12_u64_full.md"
         if prof.exists():
-            p = json.loads(prof.read_text())
-            # dram bytes per candidate from the ncu capture, times the
-            # candidates of one average launch
-            traffic = p["dram_bytes_per_candidate"] * evaluated / max(1, a.steps * (L - 1))
+            import re
+            m = re.search(r"\|\s*dram_bytes_per_candidate\s*\|\s*([0-9.eE+-]+)", prof.read_text())
+            if m:
+                # DRAM bytes per candidate from the ncu capture, times the
+                # candidates of one average spine-kernel launch
+                traffic = float(m.group(1)) * evaluated / max(1, a.steps * (L - 1))
         out = {
             "metric": "candidate-evals/s", "value": value, "unit": "candidate-evals/s",
             "n_gpus": world, "steps": a.steps, "warmup": max(a.warmup, 3),

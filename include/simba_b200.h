@@ -172,7 +172,10 @@ typedef struct {
  * is one persistent kernel whose work queue spans every active instance, and
  * an instance whose size produced a match retires at the end of the round.
  * opt->table_bytes caps each instance's value tables (0 = 8 MiB);
- * opt->budget_seconds bounds the whole batch. */
+ * opt->budget_seconds bounds the whole batch.  With opt->class_prior set it
+ * points to n x 64 priors (one row per instance, e.g. from
+ * simba_mlp_predict) and the batch is guided: each instance visits its
+ * spines by decreasing prior and retires at its first verified match. */
 int simba_solve_batch(const simba_instance *insts, int n, int max_size, const simba_options *opt,
                       simba_batch_result *results, simba_batch_stats *stats);
 

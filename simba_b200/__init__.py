@@ -217,6 +217,11 @@ def solve_batch(insts: Sequence[Instance], max_size: int, **kw):
     Each Result carries status, size, op, rank, postfix, expr, candidates and
     `seconds` = time to solution from the start of the batch."""
     n = len(insts)
+    if kw.get("class_prior") is not None:
+        cp = np.ascontiguousarray(kw["class_prior"], dtype=np.float32)
+        if cp.shape != (n, 64):
+            raise ValueError("batch class_prior must be n x 64")
+        kw["class_prior"] = cp
     arrs = [_Arrays(i) for i in insts]
     carr = (_Instance * n)(*[a.c for a in arrs])
     res = (_BatchResult * max(n, 1))()

@@ -149,6 +149,22 @@ struct TmplDesc {
   unsigned long long small_off;   // into Params::sitems
   unsigned int nitems;
   unsigned int nsmall;
+  unsigned long long bucket_off;  // guided lists: into Params::buckets
+};
+
+// Guided batch: a spine list grouped by shape class (64 buckets, each in
+// rank order) -- where each bucket's spines and units start in the list.
+struct TmplBuckets {
+  unsigned int item[65];
+  unsigned int pad;
+  unsigned long long unit[65];
+};
+
+// Guided batch: the order in which one task visits the buckets (its
+// instance's class prior, highest first) and the units before each.
+struct TaskOrder {
+  unsigned char order[64];
+  unsigned long long prefix[65];
 };
 
 template <class W>
@@ -156,6 +172,8 @@ struct Params {
   const InstDesc<W>* insts;
   const Task* tasks;        // batch mode when non-null
   const TmplDesc* tmpls;
+  const TmplBuckets* buckets;  // guided batch
+  const TaskOrder* orders;     // guided batch, one per task
   int ntasks;
   const Item* items;
   const Ctx<W>* ctxs;     // materialised contexts of fused groups
@@ -713,6 +731,20 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
           ilo = (int)td.item_off;
           ihi = (int)(td.item_off + td.nitems) - 1;
           inst = (int)tk.inst;
+          if (p.orders) {  // guided: the task's bucket order, then the bucket's spines
+            const TaskOrder& to = p.orders[lo];
+            int rl = 0, rh = 63;
+            while (rl < rh) {
+              const int mid = (rl + rh + 1) >> 1;
+              if (to.prefix[mid] <= local) rl = mid;
+              else rh = mid - 1;
+            }
+            const int b = to.order[rl];
+            const TmplBuckets& tb = p.buckets[td.bucket_off];
+            local = tb.unit[b] + (local - to.prefix[rl]);
+            ilo = (int)(td.item_off + tb.item[b]);
+            ihi = (int)(td.item_off + tb.item[b + 1]) - 1;
+          }
         }
         while (ilo < ihi) {
           const int mid = (ilo + ihi + 1) >> 1;
@@ -1568,6 +1600,7 @@ struct ItemTemplate {
   double cand = 0;           // candidates evaluated for the whole size
   bool ok = true;            // false: spines too deep, use per-rank kernel
   int id = -1;               // index of its TmplDesc on the device
+  uint64_t bucket_units[64] = {};  // guided lists: units per shape class
 };
 
 // Batched plain search: many independent instances advance size by size in
@@ -1775,17 +1808,39 @@ class Batch {
       }
       // 2. one task per active instance, pointing at its shared spine list
       tasks_.clear();
+      orders_.clear();
+      const float* priors = o_.class_prior;  // n x 64 in batch mode
+      const bool guided = priors != nullptr;
       uint64_t ctx_base = 0, units = 0;
       std::vector<int> naive_insts;
       for (int i = 0; i < n; ++i) {
         if (!active[i]) continue;
         const CountTable& ct = cts_[ct_of[i]];
         const int ul = hs_[i].unit_log2 > 0 ? std::min(hs_[i].unit_log2, 40) : 0;
-        const ItemTemplate& tp =
-            get_template(ct, std::min(T[i], size[i]), size[i], mask, ul ? 1ULL << ul : unit_target_);
+        const ItemTemplate& tp = get_template(ct, std::min(T[i], size[i]), size[i], mask,
+                                              ul ? 1ULL << ul : unit_target_, guided);
         if (!tp.ok || tp.units == 0) {
           naive_insts.push_back(i);
           continue;
+        }
+        if (guided) {  // visit the shape classes by this instance's prior
+          const float* pr = priors + (size_t)i * 64;
+          int ord[64];
+          float pb[64];
+          for (int b = 0; b < 64; ++b) {
+            ord[b] = b;
+            pb[b] = b < 8 ? std::max(pr[b], pr[32 + b]) : pr[b];
+          }
+          std::stable_sort(ord, ord + 64, [&](int a, int b) { return pb[a] > pb[b]; });
+          TaskOrder to;
+          uint64_t acc = 0;
+          for (int r = 0; r < 64; ++r) {
+            to.order[r] = (unsigned char)ord[r];
+            to.prefix[r] = acc;
+            acc += tp.bucket_units[ord[r]];
+          }
+          to.prefix[64] = acc;
+          orders_.push_back(to);
         }
         Task tk;
         tk.unit_begin = units;
@@ -1807,6 +1862,10 @@ class Batch {
         SB_CUDA(d_tdesc_.reserve(std::max<size_t>(1, tdescs_.size()) * sizeof(TmplDesc)));
         SB_CUDA(cudaMemcpyAsync(d_tdesc_.p, tdescs_.data(), tdescs_.size() * sizeof(TmplDesc),
                                 cudaMemcpyHostToDevice, stream_));
+        SB_CUDA(d_buckets_.reserve(std::max<size_t>(1, all_buckets_.size()) * sizeof(TmplBuckets)));
+        SB_CUDA(cudaMemcpyAsync(d_buckets_.p, all_buckets_.data(),
+                                all_buckets_.size() * sizeof(TmplBuckets), cudaMemcpyHostToDevice,
+                                stream_));
         tmpl_dirty_ = false;
       }
       // 3. descriptors and per-instance best
@@ -1853,6 +1912,14 @@ class Batch {
                                 cudaMemcpyHostToDevice, stream_));
         p.tasks = d_tasks_.as<Task>();
         p.ntasks = (int)tasks_.size();
+        if (guided) {
+          SB_CUDA(d_orders_.reserve(orders_.size() * sizeof(TaskOrder)));
+          SB_CUDA(cudaMemcpyAsync(d_orders_.p, orders_.data(), orders_.size() * sizeof(TaskOrder),
+                                  cudaMemcpyHostToDevice, stream_));
+          p.orders = d_orders_.as<TaskOrder>();
+          p.buckets = d_buckets_.as<TmplBuckets>();
+          p.stop_on_match = 2;  // any verified match of the size
+        }
         p.tmpls = d_tdesc_.as<TmplDesc>();
         p.items = d_items_.as<Item>();
         p.nitems = (int)all_items_.size();
@@ -1943,12 +2010,19 @@ class Batch {
   }
 
  private:
+  // Bucket of a spine in a guided list: its (primary) shape class.
+  static int bucket_of(const Item& it, int s) {
+    int a, b;
+    spine_classes(it, s, &a, &b);
+    return a < 0 ? 0 : a;
+  }
+
   const ItemTemplate& get_template(const CountTable& ct, int T, int s, uint64_t mask,
-                                   uint64_t unit_target) {
+                                   uint64_t unit_target, bool guided = false) {
     int ul = 0;
     while ((1ULL << ul) < unit_target && ul < 63) ++ul;
-    const uint64_t key =
-        ((uint64_t)ul << 24) | ((uint64_t)ct.terms << 16) | ((uint64_t)T << 8) | (uint64_t)s;
+    const uint64_t key = ((uint64_t)guided << 32) | ((uint64_t)ul << 24) |
+                         ((uint64_t)ct.terms << 16) | ((uint64_t)T << 8) | (uint64_t)s;
     auto f = templates_.find(key);
     if (f != templates_.end()) return f->second;
     ItemTemplate tp;
@@ -1979,10 +2053,17 @@ class Batch {
           if (it.lv[l].kind == 1) it.lv[l].c &= mask;
         finish_structure(it, mask);
       }
-      fuse_small(items, &tp.small, &tp.nctxs, ct, 1ULL << 22);
+      if (guided)  // fused groups stay inside one bucket
+        for (auto& it : items) it.prio = (float)bucket_of(it, s);
+      fuse_small(items, &tp.small, &tp.nctxs, ct, 1ULL << 22, guided);
       for (auto& it : items) finish_layout(it, kThreads, unit_target);
-      std::stable_sort(items.begin(), items.end(),
-                       [](const Item& a, const Item& b) { return a.base < b.base; });
+      if (guided)
+        std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) {
+          return a.prio != b.prio ? a.prio < b.prio : a.base < b.base;
+        });
+      else
+        std::stable_sort(items.begin(), items.end(),
+                         [](const Item& a, const Item& b) { return a.base < b.base; });
       for (auto& it : items) {
         tp.units += it.cblocks * it.vblocks;
         tp.cand += (double)it.nctx * (double)it.nv;
@@ -2002,6 +2083,23 @@ class Batch {
       td.nitems = (unsigned)items.size();
       td.small_off = all_small_.size();
       td.nsmall = (unsigned)tp.small.size();
+      td.bucket_off = 0;
+      if (guided) {
+        TmplBuckets tb;
+        memset(&tb, 0, sizeof(tb));
+        size_t q = 0;
+        uint64_t uacc = 0;
+        for (int b = 0; b < 64; ++b) {
+          tb.item[b] = (unsigned)q;
+          tb.unit[b] = uacc;
+          for (; q < items.size() && (int)items[q].prio == b; ++q) uacc += items[q].cblocks * items[q].vblocks;
+        }
+        tb.item[64] = (unsigned)q;
+        tb.unit[64] = uacc;
+        td.bucket_off = all_buckets_.size();
+        all_buckets_.push_back(tb);
+        for (int b = 0; b < 64; ++b) tp.bucket_units[b] = tb.unit[b + 1] - tb.unit[b];
+      }
       all_items_.insert(all_items_.end(), items.begin(), items.end());
       all_small_.insert(all_small_.end(), tp.small.begin(), tp.small.end());
       tp.id = (int)tdescs_.size();
@@ -2023,11 +2121,13 @@ class Batch {
   std::map<uint64_t, ItemTemplate> templates_;
   std::vector<Item> all_items_, all_small_;  // every spine list, concatenated
   std::vector<TmplDesc> tdescs_;
+  std::vector<TmplBuckets> all_buckets_;
+  std::vector<TaskOrder> orders_;
   bool tmpl_dirty_ = false;
   std::vector<Task> tasks_;
   std::vector<BuildJob<W>> build_jobs_;
   DevBuf d_tab_, d_smp_, d_cts_, d_best_, d_desc_, d_scal_, d_items_, d_small_, d_ctx_, d_jobs_,
-      d_tasks_, d_tdesc_;
+      d_tasks_, d_tdesc_, d_buckets_, d_orders_;
 };
 
 template <class W>
