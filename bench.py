@@ -127,11 +127,11 @@ def cpu_baseline(inst, size: int) -> dict:
     """OpenMP oracle on a bounded sample of size-`size` ranks (~10-20 s)."""
     from oracle import oracle as O
     cores = O.max_threads()
-    probe = 200_000
+    probe = 2_000_000
     t0 = time.perf_counter()
     O.scan_range(inst.inputs, inst.outputs, size, 0, probe, 64)
     rate = probe / max(time.perf_counter() - t0, 1e-6)
-    n = int(min(max(rate * 12, probe), 5e8))
+    n = int(min(max(rate * 12, probe), 2e10))  # about 12 s of CPU work
     t0 = time.perf_counter()
     ev, _, _ = O.scan_range(inst.inputs, inst.outputs, size, 0, n, 64)
     dt = time.perf_counter() - t0

@@ -1169,7 +1169,6 @@ class Search final : public SearchSession {
     if (ev0_) cudaEventDestroy(ev0_);
     if (evk_) cudaEventDestroy(evk_);
     if (ev1_) cudaEventDestroy(ev1_);
-    if (h_scal_) cudaFreeHost(h_scal_);
   }
 
   int init() {
@@ -1206,7 +1205,7 @@ class Search final : public SearchSession {
     SB_CUDA(cudaMemcpy(d_counts_.p, ct_.n, sizeof(ct_.n), cudaMemcpyHostToDevice));
     SB_CUDA(d_scal_.reserve(256));
     SB_CUDA(d_insts_.reserve(sizeof(InstDesc<W>)));
-    SB_CUDA(cudaHostAlloc(&h_scal_, 256, cudaHostAllocDefault));
+
     // table budget -> largest tabled size
     const int64_t budget = o_.table_bytes > 0 ? o_.table_bytes : (4LL << 30);
     uint64_t total = 0;
@@ -1217,13 +1216,7 @@ class Search final : public SearchSession {
       total += bytes;
       Tcap_ = t;
     }
-    if (Tcap_ < 1) Tcap_ = 1;
-    SB_CUDA(d_tab_.reserve(total + 256));
-    uint64_t off = 0;
-    for (int t = 1; t <= Tcap_; ++t) {
-      tab_off_[t] = off;
-      off += padded(ct_.n[t][8]) * sizeof(W);
-    }
+    if (Tcap_ < 1) Tcap_ = 1;  // tables are allocated when first built
     built_ = 0;
     smem_bytes_ = ((sizeof(Smem) + 15) & ~size_t(15)) +
                   (((size_t)h_.S * h_.k * sizeof(W) + 15) / 16 + ((size_t)h_.S * sizeof(W) + 15) / 16) * 16;
@@ -1272,11 +1265,12 @@ class Search final : public SearchSession {
  private:
   static uint64_t padded(uint64_t n) { return (n + 63) / 64 * 64 + 64; }
 
-  W* tab(int t) const { return reinterpret_cast<W*>(d_tab_.as<char>() + tab_off_[t]); }
+  W* tab(int t) const { return d_tabs_[t].as<W>(); }
 
   // Build V_{built+1} .. V_t (each entry one operator over smaller tables).
   int ensure_tables(int t) {
     for (int s = built_ + 1; s <= t; ++s) {
+      SB_CUDA(d_tabs_[s].reserve(padded(ct_.n[s][8]) * sizeof(W)));
       W* o = tab(s);
       if (s == 1) {
         std::vector<W> v(padded(h_.k), 0);
@@ -1580,9 +1574,9 @@ class Search final : public SearchSession {
   uint64_t alg_ops_ = 0;
   int sms_ = 0, grid_ = 0, grid_naive_ = 0;
   size_t smem_bytes_ = 0;
-  DevBuf d_in_, d_out_, d_counts_, d_scal_, d_tab_, d_items_, d_small_, d_ctx_, d_insts_;
-  void* h_scal_ = nullptr;
-  uint64_t tab_off_[kMaxSize + 1] = {};
+  DevBuf d_in_, d_out_, d_counts_, d_scal_, d_items_, d_small_, d_ctx_, d_insts_;
+  DevBuf d_tabs_[kMaxSize + 1];  // V_t, allocated when size t is first built
+  unsigned long long h_scal_[8] = {};
   int Tcap_ = 0, built_ = 0, last_T_ = 0;
 };
 
