@@ -211,6 +211,7 @@ def run_ours(a, rank: int, world: int, local_rank: int) -> None:
 
     if rank == 0:
         peak = S.int_peak(local_rank)
+        alu_peak = S.alu_peak(local_rank)
         kernel_s = kernel_ms / 1e3
         achieved = alg_ops / kernel_s if kernel_s > 0 else 0.0
         traffic = None
@@ -240,7 +241,9 @@ def run_ours(a, rank: int, world: int, local_rank: int) -> None:
                          "traffic": traffic,
                          "kernel": "spine_kernel", "kernel_ms_per_step": kernel_ms / a.steps,
                          "alg_ops_per_candidate": alg_ops / max(1, evaluated),
-                         "peak_source": "measured live: simba_int_peak (LOP3+IMAD chains)"},
+                         "peak_source": "measured live: simba_int_peak (LOP3+IMAD chains)",
+                         "alu_pipe_peak": alu_peak / 1e12,
+                         "frac_of_alu_pipe": achieved / alu_peak if alu_peak else None},
             "gpu_launches": launches,
             "clocks": clk,
         }

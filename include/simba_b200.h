@@ -70,6 +70,15 @@ typedef struct {
                             in decreasing prior and the search stops at the
                             first verified match, which has the minimal size
                             but need not have the minimum rank.  NULL = plain */
+  int32_t rank_order;    /* simba_solve only.  0: the minimum matching rank of
+                            the first operator block with a match; 1: RTid
+                            order (the reference's simba_rtid build,
+                            nocache_rtid.cu:85-95): the block's ranks are
+                            visited as (t * c) mod N, t = 0, 1, ..., and the
+                            match with the smallest t is returned; c is the
+                            smallest integer >= 2246822507 coprime to N, so
+                            every rank is visited exactly once            */
+  int32_t reserved;
 } simba_options;
 
 typedef struct {
@@ -149,7 +158,10 @@ typedef struct {
   int32_t reserved;
   uint64_t rank;
   char postfix[64];
-  double seconds;        /* time to solution, from the start of the batch        */
+  double seconds;        /* time to solution on the device clock, from the batch's
+                            first kernel: the first verified match (guided) or
+                            the end of the instance's last unit (plain); for
+                            unsolved instances the host time of retirement     */
   uint64_t candidates;   /* reference-rule candidates of this instance           */
 } simba_batch_result;
 
@@ -160,7 +172,7 @@ typedef struct {
   double alg_ops;        /* integer lane-operations of the candidates evaluated  */
   uint64_t candidates;
   uint64_t evaluated;
-  int32_t rounds;        /* one persistent launch per round (size step)          */
+  int32_t rounds;        /* one persistent launch per round                      */
   int32_t launches;
   int32_t solved;
   int32_t reserved;
@@ -169,13 +181,18 @@ typedef struct {
 /* Batched plain search of n independent instances of one word width (no
  * counterpart in the reference, which runs one process per instance,
  * run_all.sh:20-43).  Instances advance size by size in rounds; each round
- * is one persistent kernel whose work queue spans every active instance, and
- * an instance whose size produced a match retires at the end of the round.
+ * is one persistent kernel whose work queue spans the instances of the
+ * round, and an instance whose size produced a match retires.  Rounds are
+ * cost-ordered: an instance searches its next size in a round when the
+ * candidates it will then have swept are within 64x (environment
+ * SIMBA_ROUND_GROWTH; 0 = every active instance) of the cheapest active
+ * instance's, and the round's queue runs the cheapest instances first.
  * opt->table_bytes caps each instance's value tables (0 = 8 MiB);
  * opt->budget_seconds bounds the whole batch.  With opt->class_prior set it
  * points to n x 64 priors (one row per instance, e.g. from
- * simba_mlp_predict) and the batch is guided: each instance visits its
- * spines by decreasing prior and retires at its first verified match. */
+ * simba_mlp_predict) and the batch is guided: the queue holds one entry per
+ * (instance, shape class), ordered by prior per unit of work across the
+ * round, and an instance retires at its first verified match. */
 int simba_solve_batch(const simba_instance *insts, int n, int max_size, const simba_options *opt,
                       simba_batch_result *results, simba_batch_stats *stats);
 
@@ -228,6 +245,9 @@ void simba_instance_free(simba_instance *inst);
  * denominator of the search kernels' roofline (no counterpart in the
  * reference, which reports no roofline). */
 int simba_int_peak(int device, double *lane_ops_per_s);
+/* The same with LOP3 only: the rate of the ALU pipe alone, which bounds
+ * kernels whose instructions are all bitwise/compare operations. */
+int simba_alu_peak(int device, double *lane_ops_per_s);
 
 /* Shape class of an expression (the guided search's unit of priority and
  * the label the proposal learns): 8 * root operator + min(left operand size,

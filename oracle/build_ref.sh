@@ -5,6 +5,7 @@
 # except the architecture.  Outputs go to oracle/_ref/ only.
 #
 #   oracle/_ref/simba_nocache   <- simba/src/nocache.cu + simba/src/instance.cpp
+#   oracle/_ref/simba_rtid      <- simba/src/nocache_rtid.cu + simba/src/instance.cpp
 #   oracle/_ref/vfb_full_cache  <- vfb/src/full-cache.cu
 #
 # Usage: oracle/build_ref.sh [path-to-reference]   (default /root/reference)
@@ -22,6 +23,10 @@ fi
 if [ ! -x "$OUT/simba_nocache" ] || [ "$REF/simba/src/nocache.cu" -nt "$OUT/simba_nocache" ]; then
   "$NVCC" -O2 -std=c++20 --extended-lambda -arch="$ARCH" \
     "$REF/simba/src/nocache.cu" "$REF/simba/src/instance.cpp" -o "$OUT/simba_nocache"
+fi
+if [ ! -x "$OUT/simba_rtid" ] || [ "$REF/simba/src/nocache_rtid.cu" -nt "$OUT/simba_rtid" ]; then
+  "$NVCC" -O2 -std=c++20 --extended-lambda -arch="$ARCH" \
+    "$REF/simba/src/nocache_rtid.cu" "$REF/simba/src/instance.cpp" -o "$OUT/simba_rtid"
 fi
 if [ ! -x "$OUT/vfb_full_cache" ] || [ "$REF/vfb/src/full-cache.cu" -nt "$OUT/vfb_full_cache" ]; then
   "$NVCC" -O2 -std=c++20 -I"$REF/vfb/include" -I"$REF/vfb/src" --extended-lambda -arch="$ARCH" \

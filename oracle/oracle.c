@@ -255,6 +255,109 @@ int orc_search(int bits, int k, int S, const uint64_t *in, const uint64_t *out, 
 }
 
 /* ---------------------------------------------------------------------------
+ * RTid order: simba/src/nocache_rtid.cu:85-95.  Thread t of an operator
+ * block of N ranks (grid ceil(N/1024)*1024) evaluates rank (t * C) % N with
+ * C = 2246822507 in 64-bit arithmetic.  mode 1 restates exactly that map,
+ * over every launched t (the reference's own visiting set: C = 15809 *
+ * 142123 is not coprime to every N, and t * C wraps for t > 8.2e9, so some
+ * ranks may be skipped and others visited twice).  mode 0 is the bijection
+ * the product implements: multiplier c = the smallest c >= C with
+ * gcd(c, N) = 1, exact product, t in [0, N).  Both return the match with the
+ * smallest t (the reference returns whichever thread wins its atomicCAS).
+ * ------------------------------------------------------------------------- */
+static uint64_t orc_mulmod(uint64_t a, uint64_t b, uint64_t n) {
+  return (uint64_t)(((unsigned __int128)a * b) % n);
+}
+
+static uint64_t orc_gcd(uint64_t a, uint64_t b) {
+  while (b) {
+    uint64_t t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+uint64_t orc_rtid_multiplier(uint64_t n) {
+  uint64_t c = 2246822507ULL;
+  while (n > 1 && orc_gcd(c % n, n) != 1) ++c;
+  return c;
+}
+
+static uint64_t rtid_map(uint64_t t, uint64_t n, uint64_t c, int mode) {
+  if (mode == 1) return (t * 2246822507ULL) % n; /* wraps mod 2^64 like the reference */
+  return orc_mulmod(t, c, n);
+}
+
+int orc_search_rtid(int bits, int k, int S, const uint64_t *in, const uint64_t *out, int max_size,
+                    int include_edges, int mode, int nth, orc_result *res) {
+  memset(res, 0, sizeof(*res));
+  if (max_size > ORC_MAX_SIZE || k > ORC_MAX_TERMS || k < 1 || S < 1 || mode < 0 || mode > 1)
+    return -2;
+  uint64_t t[(ORC_MAX_SIZE + 1) * 9];
+  if (orc_count_table(max_size, k, t) != 0) return -3;
+  if (nth <= 0) nth = orc_max_threads();
+  const uint64_t m = wmask(bits);
+  if (include_edges) {
+    for (int v = 0; v < k; ++v) {
+      res->candidates++;
+      res->per_size[1]++;
+      int ok = 1;
+      for (int i = 0; i < S && ok; ++i) ok = (in[(size_t)i * k + v] & m) == (out[i] & m);
+      if (ok) {
+        res->found = 1;
+        res->size = 1;
+        res->op = 8;
+        res->rank = (uint64_t)v;
+        res->postfix[0] = (char)('0' + v);
+        return 1;
+      }
+    }
+  }
+  const int last = include_edges ? max_size : max_size - 1;
+  for (int s = 2; s <= last; ++s) {
+    uint64_t off = 0;
+    for (int op = 0; op < 8; ++op) {
+      const uint64_t N = t[s * 9 + op];
+      res->candidates += N;
+      res->per_size[s] += N;
+      if (!N) continue;
+      const uint64_t c = orc_rtid_multiplier(N);
+      const uint64_t T = mode == 1 ? (N + 1023) / 1024 * 1024 : N;
+      const int64_t nchunks = (int64_t)((T + ORC_CHUNK - 1) / ORC_CHUNK);
+      uint64_t best = ~0ULL;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nth)
+#endif
+      for (int64_t ch = 0; ch < nchunks; ++ch) {
+        const uint64_t a = (uint64_t)ch * ORC_CHUNK;
+        const uint64_t b = a + ORC_CHUNK < T ? a + ORC_CHUNK : T;
+        if (a > __atomic_load_n(&best, __ATOMIC_RELAXED)) continue;
+        char p[ORC_MAX_SIZE + 1];
+        for (uint64_t x = a; x < b; ++x) {
+          orc_unrank(off + rtid_map(x, N, c, mode), s, t, p);
+          if (orc_check(p, s, bits, k, S, in, out)) {
+            atomic_min_u64(&best, x);
+            break;
+          }
+        }
+      }
+      if (best != ~0ULL) {
+        res->found = 1;
+        res->size = s;
+        res->op = op;
+        res->rank = off + rtid_map(best, N, c, mode);
+        orc_unrank(res->rank, s, t, res->postfix);
+        res->postfix[s] = 0;
+        return 1;
+      }
+      off += N;
+    }
+  }
+  return 0;
+}
+
+/* ---------------------------------------------------------------------------
  * VFB: bottom-up enumeration with observational-equivalence dedup.
  * vfb/src/full-cache.cu:665-774 (driver), :568-663 (per-operator loops),
  * :333-372 (candidate order, Minus also tries the swapped pair), :460-472

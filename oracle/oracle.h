@@ -55,6 +55,10 @@ int orc_check(const char *postfix, int len, int word_bits, int n_terms, int n_sa
 int orc_search(int word_bits, int n_terms, int n_samples, const uint64_t *inputs,
                const uint64_t *outputs, int max_size, int include_edges, int n_threads,
                orc_result *res);
+int orc_search_rtid(int word_bits, int n_terms, int n_samples, const uint64_t *inputs,
+                    const uint64_t *outputs, int max_size, int include_edges, int mode,
+                    int n_threads, orc_result *res);
+uint64_t orc_rtid_multiplier(uint64_t n);
 int64_t orc_scan_range(int word_bits, int n_terms, int n_samples, const uint64_t *inputs,
                        const uint64_t *outputs, int size, uint64_t rank_lo, uint64_t rank_hi,
                        int n_threads, uint64_t *min_rank, uint64_t *n_hits);

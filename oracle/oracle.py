@@ -53,6 +53,10 @@ def lib():
         L.orc_check.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, u64p, u64p]
         L.orc_search.argtypes = [C.c_int, C.c_int, C.c_int, u64p, u64p, C.c_int, C.c_int,
                                  C.c_int, C.POINTER(OrcResult)]
+        L.orc_search_rtid.argtypes = [C.c_int, C.c_int, C.c_int, u64p, u64p, C.c_int, C.c_int,
+                                      C.c_int, C.c_int, C.c_void_p]
+        L.orc_rtid_multiplier.argtypes = [C.c_uint64]
+        L.orc_rtid_multiplier.restype = C.c_uint64
         L.orc_scan_range.argtypes = [C.c_int, C.c_int, C.c_int, u64p, u64p, C.c_int,
                                      C.c_uint64, C.c_uint64, C.c_int, u64p, u64p]
         L.orc_scan_range.restype = C.c_int64
@@ -114,6 +118,28 @@ def search(inputs, outputs, max_size: int, word_bits: int = 64, include_edges: b
     return {"found": bool(res.found), "size": res.size, "op": res.op, "rank": res.rank,
             "postfix": res.postfix[: res.size].decode() if res.found else "",
             "candidates": res.candidates, "per_size": list(res.per_size)}
+
+
+def search_rtid(inputs, outputs, max_size: int, word_bits: int = 64, include_edges: bool = False,
+                reference_map: bool = False, n_threads: int = 0) -> dict:
+    """RTid-order search: the match with the smallest thread position t of
+    the first operator block with a match.  reference_map=True restates the
+    reference's own map (64-bit wrap, C not coprime to every N)."""
+    ins = _u64(inputs)
+    outs = _u64(outputs)
+    S, k = ins.shape
+    res = OrcResult()
+    rc = lib().orc_search_rtid(word_bits, k, S, _p(ins), _p(outs), max_size, int(include_edges),
+                               int(reference_map), n_threads, C.byref(res))
+    if rc < 0:
+        raise ValueError(f"oracle rtid search failed ({rc})")
+    return {"found": bool(res.found), "size": res.size, "op": res.op, "rank": res.rank,
+            "postfix": res.postfix[: res.size].decode() if res.found else "",
+            "candidates": res.candidates, "per_size": list(res.per_size)}
+
+
+def rtid_multiplier(n: int) -> int:
+    return int(lib().orc_rtid_multiplier(C.c_uint64(n)))
 
 
 def scan_range(inputs, outputs, size: int, lo: int, hi: int, word_bits: int = 64,

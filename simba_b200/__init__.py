@@ -43,7 +43,8 @@ class _Options(C.Structure):
                 ("engine", C.c_int32), ("budget_seconds", C.c_double),
                 ("table_bytes", C.c_int64), ("stream", C.c_uint64),
                 ("vfb_cache_rows", C.c_int64), ("vfb_reference_dedup", C.c_int32),
-                ("unit_log2", C.c_int32), ("class_prior", C.POINTER(C.c_float))]
+                ("unit_log2", C.c_int32), ("class_prior", C.POINTER(C.c_float)),
+                ("rank_order", C.c_int32), ("reserved", C.c_int32)]
 
 
 class _BatchResult(C.Structure):
@@ -114,6 +115,7 @@ def lib():
     L.simba_status_string.argtypes = [C.c_int]
     L.simba_device_count.restype = C.c_int
     L.simba_int_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    L.simba_alu_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
     L.vfb_solve.argtypes = [P(_Instance), C.c_int, P(_Options), P(_VfbResult)]
     L.simba_solve_noalloc.argtypes = [P(_Instance), C.c_int, P(_Options), P(_Result)]
     L.simba_solve_batch.argtypes = [P(_Instance), C.c_int, C.c_int, P(_Options),
@@ -168,7 +170,7 @@ class _Arrays:
 
 def _opts(device=0, complete=False, verbose=False, naive=False, budget=0.0,
           table_bytes=0, stream=0, cache_rows=0, reference_dedup=False,
-          unit_log2=0, class_prior=None) -> _Options:
+          unit_log2=0, class_prior=None, rtid=False) -> _Options:
     o = _Options()
     o.device = device
     o.size_range = 1 if complete else 0
@@ -180,6 +182,7 @@ def _opts(device=0, complete=False, verbose=False, naive=False, budget=0.0,
     o.vfb_cache_rows = int(cache_rows)
     o.vfb_reference_dedup = 1 if reference_dedup else 0
     o.unit_log2 = int(unit_log2)
+    o.rank_order = 1 if rtid else 0
     if class_prior is not None:  # the caller keeps the array alive for the call
         o.class_prior = class_prior.ctypes.data_as(C.POINTER(C.c_float))
     return o
@@ -215,7 +218,9 @@ def solve_batch(insts: Sequence[Instance], max_size: int, **kw):
     """Batched plain search: returns (per-instance Result list, stats dict).
 
     Each Result carries status, size, op, rank, postfix, expr, candidates and
-    `seconds` = time to solution from the start of the batch."""
+    `seconds` = time to solution on the device clock from the batch's first
+    kernel (guided: the first verified match; plain: the end of the
+    instance's last work unit)."""
     n = len(insts)
     if kw.get("class_prior") is not None:
         cp = np.ascontiguousarray(kw["class_prior"], dtype=np.float32)
@@ -360,6 +365,13 @@ def int_peak(device: int = 0) -> float:
     """Measured int32 lane-operations per second of the device."""
     v = C.c_double()
     _check(lib().simba_int_peak(device, C.byref(v)))
+    return v.value
+
+
+def alu_peak(device: int = 0) -> float:
+    """Measured ALU-pipe (LOP3) lane-operations per second of the device."""
+    v = C.c_double()
+    _check(lib().simba_alu_peak(device, C.byref(v)))
     return v.value
 
 

@@ -5,6 +5,7 @@ arch=compute_100a,code=sm_100a``) and links, in-tree:
 
     simba_b200/libsimba_b200.so   the C ABI of include/simba_b200.h
     simba_b200/bin/simba          drop-in for the reference `simba` executable
+    simba_b200/bin/simba_rtid     drop-in for the reference `simba_rtid` executable
     simba_b200/bin/vfb            drop-in for the reference `vfb` executable
 
 Usage: python -m simba_b200.build [--force] [--verbose]
@@ -87,14 +88,16 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if force or jobs or _newer(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", LIB] + objs
              + ["-cudart", "static", "-lpthread", "-ldl", "-lrt"], verbose)
-    for cli, name in (("cli_simba.cpp", "simba"), ("cli_vfb.cpp", "vfb")):
+    for cli, name, defs in (("cli_simba.cpp", "simba", []),
+                            ("cli_simba.cpp", "simba_rtid", ["-DSIMBA_CLI_RTID=1"]),
+                            ("cli_vfb.cpp", "vfb", [])):
         s = CSRC / cli
         if not s.exists():
             continue
         out = BIN / name
         if force or _newer(out, [s, LIB] + hdrs):
-            _run([_host_cxx()] + CXX_FLAGS + [s, "-o", out, f"-L{PKG}", "-lsimba_b200",
-                                               "-Wl,-rpath,$ORIGIN/.."], verbose)
+            _run([_host_cxx()] + CXX_FLAGS + defs + [s, "-o", out, f"-L{PKG}", "-lsimba_b200",
+                                                      "-Wl,-rpath,$ORIGIN/.."], verbose)
     return LIB
 
 

@@ -144,6 +144,7 @@ static EngineOptions to_opts(const simba_options* o) {
     e.stream = o->stream;
     e.unit_log2 = o->unit_log2;
     e.class_prior = o->class_prior;
+    e.rank_order = o->rank_order;
   }
   return e;
 }
@@ -277,6 +278,12 @@ int simba_solve(const simba_instance* inst, int max_size, const simba_options* o
     result->status = rc;
     return rc;
   }
+  if (opt && (opt->rank_order < 0 || opt->rank_order > 1 ||
+              (opt->rank_order == 1 && (opt->class_prior || opt->engine == 1)))) {
+    set_last_error("rank_order must be 0, or 1 for the plain spine search");
+    result->status = SIMBA_E_ARG;
+    return SIMBA_E_ARG;
+  }
   SearchSession* s = nullptr;
   rc = make_search_session(h, to_opts(opt), &s);
   if (rc) {
@@ -307,6 +314,11 @@ int simba_solve_noalloc(const simba_instance* inst, int max_size, const simba_op
     result->status = rc;
     return rc;
   }
+  if (opt && opt->rank_order != 0) {
+    set_last_error("rank_order 1 (RTid) is supported by simba_solve only");
+    result->status = SIMBA_E_ARG;
+    return SIMBA_E_ARG;
+  }
   SolveOutcome oc;
   rc = solve_static(h, max_size, to_opts(opt), &oc);
   const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -321,6 +333,10 @@ int simba_solve_noalloc(const simba_instance* inst, int max_size, const simba_op
 int simba_solve_batch(const simba_instance* insts, int n, const int max_size_arg,
                       const simba_options* opt, simba_batch_result* results, simba_batch_stats* stats) {
   if (!insts || n < 0 || !results) return SIMBA_E_ARG;
+  if (opt && opt->rank_order != 0) {
+    set_last_error("rank_order 1 (RTid) is supported by simba_solve only");
+    return SIMBA_E_ARG;
+  }
   const auto t0 = std::chrono::steady_clock::now();
   std::vector<HostInstance> hs(n);
   for (int i = 0; i < n; ++i) {
@@ -363,6 +379,10 @@ int simba_session_create(const simba_instance* inst, const simba_options* opt,
                          simba_session** session) {
   if (!session) return SIMBA_E_ARG;
   *session = nullptr;
+  if (opt && opt->rank_order != 0) {
+    set_last_error("rank_order 1 (RTid) is supported by simba_solve only");
+    return SIMBA_E_ARG;
+  }
   auto* ss = new simba_session();
   int rc = to_host(inst, &ss->h);
   if (!rc) rc = make_search_session(ss->h, to_opts(opt), &ss->s);
@@ -631,6 +651,11 @@ int simba_mlp_get_params(simba_mlp* mlp, float* params) {
 int simba_mlp_set_params(simba_mlp* mlp, const float* params) {
   if (!mlp || !params) return SIMBA_E_ARG;
   return mlp_set_params(mlp->m, params);
+}
+
+int simba_alu_peak(int device, double* lane_ops_per_s) {
+  if (!lane_ops_per_s) return SIMBA_E_ARG;
+  return measure_alu_peak(device, lane_ops_per_s);
 }
 
 const char* simba_version(void) { return "simba_b200 0.1 (sm_100a)"; }

@@ -8,6 +8,9 @@
 //   --complete     also search size 1 and size maxLen
 //   --naive        one thread per rank instead of the tabled engine
 //   --verbose      per-size progress on stderr
+//   --rtid         RTid order (the reference's simba_rtid build); the same
+//                  source built with SIMBA_CLI_RTID=1 is the simba_rtid
+//                  executable, for which this is the default
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -22,6 +25,9 @@
 int main(int argc, char* argv[]) {
   simba_options opt;
   memset(&opt, 0, sizeof(opt));
+#if defined(SIMBA_CLI_RTID) && SIMBA_CLI_RTID
+  opt.rank_order = 1;
+#endif
   std::vector<char*> pos;
   pos.push_back(argv[0]);
   for (int i = 1; i < argc; ++i) {
@@ -29,6 +35,7 @@ int main(int argc, char* argv[]) {
     else if (!strcmp(argv[i], "--complete")) opt.size_range = 1;
     else if (!strcmp(argv[i], "--naive")) opt.engine = 1;
     else if (!strcmp(argv[i], "--verbose")) opt.verbose = 1;
+    else if (!strcmp(argv[i], "--rtid")) opt.rank_order = 1;
     else pos.push_back(argv[i]);
   }
   if (pos.size() != 3) {

@@ -31,6 +31,7 @@ struct EngineOptions {
   uint64_t stream = 0;       // caller's cudaStream_t, 0 = own stream
   int unit_log2 = 0;         // log2 candidates per work unit, 0 = 22
   const float* class_prior = nullptr;  // guided search: 64 shape-class priors
+  int rank_order = 0;        // 0 rank order, 1 RTid order (single-instance solve only)
 };
 
 // Per-solve outcome filled by the engines (capi.cpp formats the strings).
@@ -124,6 +125,7 @@ int mlp_set_params(Mlp* m, const float* h);
 int read_instance_json(const std::string& path, HostInstance* h);
 
 int measure_int_peak(int device, double* lane_ops_per_s);
+int measure_alu_peak(int device, double* lane_ops_per_s);
 
 struct VfbOutcome {
   int status = SIMBA_NOT_FOUND;

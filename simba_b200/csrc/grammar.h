@@ -142,6 +142,77 @@ SB_HD void unrank(uint64_t rank, int size, const uint64_t (*n)[kCols], char* out
   }
 }
 
+// (a * b) mod n for any 64-bit a, b < n: shift-and-add, so it needs no
+// 128-bit division (used only when a match is recorded, never per candidate).
+SB_HD uint64_t mulmod64(uint64_t a, uint64_t b, uint64_t n) {
+  uint64_t r = 0;
+  a %= n;
+  b %= n;
+  while (b) {
+    if (b & 1) {
+      const uint64_t t = r + a;
+      r = (t < r || t >= n) ? t - n : t;
+    }
+    const uint64_t d = a + a;
+    a = (d < a || d >= n) ? d - n : d;
+    b >>= 1;
+  }
+  return r;
+}
+
+// RTid order (the simba_rtid build, nocache_rtid.cu:85-95): position t of
+// an operator block of N ranks visits the rank (t * C) mod N of the block,
+// C = 2246822507.  That C = 15809 * 142123, and t * C wraps 64 bits for
+// t > 8.2e9, so the reference's map misses ranks for some N; here the
+// multiplier is the smallest c >= C coprime to N, and the product is taken
+// exactly, which makes the order a bijection of the block.
+constexpr uint64_t kRtidMultiplier = 2246822507ULL;
+
+inline uint64_t gcd64(uint64_t a, uint64_t b) {
+  while (b) {
+    const uint64_t t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+inline uint64_t rtid_multiplier(uint64_t n) {
+  uint64_t c = kRtidMultiplier;
+  while (n > 1 && gcd64(c % n, n) != 1) ++c;
+  return c;
+}
+
+// Inverse of c modulo n (gcd(c, n) = 1), by the extended Euclidean algorithm.
+inline uint64_t inverse_mod(uint64_t c, uint64_t n) {
+  if (n <= 1) return 0;
+  __int128 t = 0, nt = 1, r = (__int128)n, nr = (__int128)(c % n);
+  while (nr != 0) {
+    const __int128 q = r / nr, a = t - q * nt, b = r - q * nr;
+    t = nt;
+    nt = a;
+    r = nr;
+    nr = b;
+  }
+  if (t < 0) t += (__int128)n;
+  return (uint64_t)t;
+}
+
+// RTid position (as off + t) of `rank` in its operator block of size s, and
+// back.  Keys of one block lie in the block's rank interval, so the minimum
+// key of a size sits in its first operator block with a match.
+inline uint64_t rtid_key(const uint64_t (*n)[kCols], int s, uint64_t rank) {
+  const int op = op_of_rank(n, s, rank);
+  const uint64_t off = op_offset(n, s, op), N = n[s][op];
+  return off + mulmod64(rank - off, inverse_mod(rtid_multiplier(N), N), N);
+}
+
+inline uint64_t rtid_rank(const uint64_t (*n)[kCols], int s, uint64_t key) {
+  const int op = op_of_rank(n, s, key);
+  const uint64_t off = op_offset(n, s, op), N = n[s][op];
+  return off + mulmod64(key - off, rtid_multiplier(N), N);
+}
+
 // postfix -> rank (inverse of unrank), used to check the bijection and to
 // locate a known expression in the rank space.  Returns false on a malformed
 // string or if a binary node's split is not enumerated (commutative with

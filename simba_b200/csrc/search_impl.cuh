@@ -43,7 +43,9 @@
 #include <map>
 #include <cstdio>
 #include <cstddef>
+#include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <vector>
 
@@ -128,10 +130,14 @@ struct alignas(16) InstDesc {
   const W* out;                     // S words, 16-byte padded
   const unsigned long long* counts; // (kMaxSize+1) x kCols count table
   unsigned long long* best;         // minimum verified matching rank
+  unsigned long long* ns;           // batch, or null: [0] first verified match,
+                                    // [1] last unit that ran (globaltimer ns)
   W target;                         // output on sample 0
   int size;
   int S, K;
-  int pad[3];
+  int rtid;                         // 1: best holds RTid keys (positions), not ranks
+  int pad[2];
+  unsigned long long rt_inv[8];     // RTid: inverse multiplier of each operator block
 };
 
 // Batch mode: one instance's search of one size, pointing at a shared spine
@@ -139,9 +145,11 @@ struct alignas(16) InstDesc {
 // same (terminals, tabled size, size, unit size).
 struct Task {
   unsigned long long unit_begin;  // first global unit of this task
-  unsigned long long ctx_base;    // first materialised context of this task
+  unsigned long long ctx_base;    // first materialised context of the instance
   unsigned int inst;
   unsigned int tmpl;
+  int bucket;                     // guided: the one shape-class bucket covered; -1: whole list
+  int pad;
 };
 
 struct TmplDesc {
@@ -160,20 +168,12 @@ struct TmplBuckets {
   unsigned long long unit[65];
 };
 
-// Guided batch: the order in which one task visits the buckets (its
-// instance's class prior, highest first) and the units before each.
-struct TaskOrder {
-  unsigned char order[64];
-  unsigned long long prefix[65];
-};
-
 template <class W>
 struct Params {
   const InstDesc<W>* insts;
   const Task* tasks;        // batch mode when non-null
   const TmplDesc* tmpls;
   const TmplBuckets* buckets;  // guided batch
-  const TaskOrder* orders;     // guided batch, one per task
   int ntasks;
   const Item* items;
   const Ctx<W>* ctxs;     // materialised contexts of fused groups
@@ -184,6 +184,7 @@ struct Params {
   unsigned long long* evaluated;
   unsigned long long* start_ns;
   int* flags;  // [0] budget expired, [1] inversion failure, [2] queue overflows
+  unsigned long long* hits;  // sample-0 matches sent to verification (may be null)
   unsigned long long total_units;
   unsigned long long unit_offset;  // this shard's first unit (multi-GPU)
   unsigned long long unit_stride;  // number of shards (0 is read as 1)
@@ -353,6 +354,39 @@ __device__ bool thread_verify(const InstDesc<W>& d, const Smem& sm, const W* s_i
   return true;
 }
 
+// The quantity whose minimum is the answer: the rank, or in RTid order the
+// rank's position off + t in its operator block (t = (rank - off) / C mod N).
+template <class W>
+__device__ __forceinline__ unsigned long long match_key(const InstDesc<W>& d, unsigned long long rank) {
+  if (!d.rtid) return rank;
+  const unsigned long long* c = d.counts + (size_t)d.size * kCols;
+  unsigned long long off = 0;
+  int op = 0;
+  while (op < 7 && rank - off >= c[op]) off += c[op++];
+  return off + mulmod64(rank - off, d.rt_inv[op], c[op]);
+}
+
+// RTid: end of the operator block that holds `key`; spines starting there
+// or later can only give larger keys.
+template <class W>
+__device__ __forceinline__ unsigned long long rtid_block_end(const InstDesc<W>& d, unsigned long long key) {
+  const unsigned long long* c = d.counts + (size_t)d.size * kCols;
+  unsigned long long end = 0;
+  for (int op = 0; op < 8; ++op) {
+    end += c[op];
+    if (key < end) break;
+  }
+  return end;
+}
+
+// Record a verified match: the minimum rank (key), and in batch mode the
+// time of the instance's first match.
+template <class W>
+__device__ __forceinline__ void note_match(const InstDesc<W>& d, unsigned long long rank) {
+  const unsigned long long prev = atomicMin(d.best, match_key<W>(d, rank));
+  if (prev == ~0ULL && d.ns) atomicCAS(d.ns, 0ULL, globaltimer_ns());
+}
+
 // Warp-cooperative verification of the queued sample-0 matches: lane i
 // checks samples i, i+32, ...; a ballot after each group of 32 samples
 // rejects the candidate at the first mismatch.
@@ -365,7 +399,7 @@ __device__ void verify_queue(const InstDesc<W>& d, Smem& sm, const W* s_in, cons
     unsigned long long cur = 0;
     if (lane == 0) cur = *(volatile unsigned long long*)d.best;
     cur = __shfl_sync(0xffffffffu, cur, 0);
-    if (rank >= cur) continue;
+    if (match_key<W>(d, rank) >= cur) continue;
     char* post = sm.post[warp];
     if (lane == 0) unrank(rank, d.size, (const uint64_t(*)[kCols])sm.counts, post);
     __syncwarp();
@@ -376,7 +410,7 @@ __device__ void verify_queue(const InstDesc<W>& d, Smem& sm, const W* s_in, cons
       if (i < d.S) ok = eval_postfix<W>(post, d.size, s_in + i * d.K) == s_out[i];
       if (__ballot_sync(0xffffffffu, !ok)) { all_ok = false; break; }
     }
-    if (all_ok && lane == 0) atomicMin(d.best, rank);
+    if (all_ok && lane == 0) note_match<W>(d, rank);
     __syncwarp();
   }
 }
@@ -406,7 +440,7 @@ __device__ __forceinline__ void push_hit(const Params<W>& p, const InstDesc<W>& 
     sm.queue[i] = rank;
   } else {
     atomicAdd(&p.flags[2], 1);
-    if (thread_verify<W>(d, sm, s_in, s_out, rank)) atomicMin(d.best, rank);
+    if (thread_verify<W>(d, sm, s_in, s_out, rank)) note_match<W>(d, rank);
   }
 }
 
@@ -731,17 +765,10 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
           ilo = (int)td.item_off;
           ihi = (int)(td.item_off + td.nitems) - 1;
           inst = (int)tk.inst;
-          if (p.orders) {  // guided: the task's bucket order, then the bucket's spines
-            const TaskOrder& to = p.orders[lo];
-            int rl = 0, rh = 63;
-            while (rl < rh) {
-              const int mid = (rl + rh + 1) >> 1;
-              if (to.prefix[mid] <= local) rl = mid;
-              else rh = mid - 1;
-            }
-            const int b = to.order[rl];
+          if (tk.bucket >= 0) {  // guided: one shape-class bucket of the list
+            const int b = tk.bucket;
             const TmplBuckets& tb = p.buckets[td.bucket_off];
-            local = tb.unit[b] + (local - to.prefix[rl]);
+            local += tb.unit[b];
             ilo = (int)(td.item_off + tb.item[b]);
             ihi = (int)(td.item_off + tb.item[b + 1]) - 1;
           }
@@ -756,9 +783,14 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
         sm.unit_local = local - p.items[ilo].unit_begin;
         const Item& nx = p.items[ilo];
         if (inst < 0) inst = (int)nx.inst;
-        const unsigned long long cur = *(volatile unsigned long long*)p.insts[inst].best;
-        // 1: minimum rank (skip spines above the best match); 2: any match
-        sm.skip = p.stop_on_match == 1 ? nx.base > cur : (p.stop_on_match == 2 && cur != ~0ULL);
+        const InstDesc<W>& di = p.insts[inst];
+        const unsigned long long cur = *(volatile unsigned long long*)di.best;
+        // 1: minimum rank (skip spines above the best match; in RTid order,
+        // spines past the best match's operator block); 2: any match
+        if (p.stop_on_match == 1)
+          sm.skip = di.rtid ? (cur != ~0ULL && nx.base >= rtid_block_end<W>(di, cur)) : nx.base > cur;
+        else
+          sm.skip = p.stop_on_match == 2 && cur != ~0ULL;
       }
     }
     __syncthreads();
@@ -797,6 +829,8 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
     if (sm.qn > 0) verify_queue<W>(d, sm, s_in, s_out);
     __syncthreads();
     if (threadIdx.x == 0) {
+      if (!sm.skip && d.ns) atomicMax(d.ns + 1, globaltimer_ns());
+      if (p.hits && sm.qn) atomicAdd(p.hits, (unsigned long long)sm.qn);
       sm.qn = 0;
       sm.item_idx = ni;
       sm.task_idx = nt;
@@ -821,7 +855,7 @@ __global__ void __launch_bounds__(kThreads) naive_kernel(Params<W> p, unsigned l
   char post[kMaxSize + 1];
   for (unsigned long long r = lo + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; r < hi;
        r += stride) {
-    if (p.stop_on_match && r > *(volatile unsigned long long*)d.best) break;
+    if (p.stop_on_match && !d.rtid && r > *(volatile unsigned long long*)d.best) break;
     if ((count & 1023) == 0 && p.budget_ns && globaltimer_ns() - *p.start_ns > p.budget_ns) {
       atomicOr(&p.flags[0], 1);
       break;
@@ -831,9 +865,11 @@ __global__ void __launch_bounds__(kThreads) naive_kernel(Params<W> p, unsigned l
     if (eval_postfix<W>(post, d.size, s_in) != s_out[0]) continue;
     bool ok = true;
     for (int i = 1; i < d.S && ok; ++i) ok = eval_postfix<W>(post, d.size, s_in + i * d.K) == s_out[i];
-    if (ok) atomicMin(d.best, r);
+    if (ok) note_match<W>(d, r);
   }
   atomicAdd(p.evaluated, count);
+  __syncthreads();
+  if (threadIdx.x == 0 && d.ns) atomicMax(d.ns + 1, globaltimer_ns());
 }
 
 template <class W>
@@ -1319,6 +1355,10 @@ class Search final : public SearchSession {
     d.size = s;
     d.S = h_.S;
     d.K = h_.k;
+    d.rtid = o_.rank_order == 1 && s > 1;
+    if (d.rtid)
+      for (int op = 0; op < 8; ++op)
+        if (ct_.n[s][op]) d.rt_inv[op] = inverse_mod(rtid_multiplier(ct_.n[s][op]), ct_.n[s][op]);
     cudaMemcpyAsync(d_insts_.p, &d, sizeof(d), cudaMemcpyHostToDevice, stream_);
     Params<W> p;
     memset(&p, 0, sizeof(p));
@@ -1327,6 +1367,7 @@ class Search final : public SearchSession {
     p.evaluated = sc + 2;
     p.start_ns = sc + 3;
     p.flags = reinterpret_cast<int*>(sc + 4);
+    p.hits = sc + 6;
     p.maxS = h_.S;
     p.maxK = h_.k;
     p.budget_ns = o_.budget_s > 0 ? (unsigned long long)(o_.budget_s * 1e9) : 0;
@@ -1475,8 +1516,9 @@ class Search final : public SearchSession {
       return SIMBA_E_INTERNAL;
     }
     if (o_.verbose)
-      fprintf(stderr, "size %2d | %s | items %zu | evaluated %llu | %.3f ms\n", s,
-              use_naive ? "naive" : "spine", items.size(), (unsigned long long)hs[2], e);
+      fprintf(stderr, "size %2d | %s | items %zu | evaluated %llu | sample-0 hits %llu | %.3f ms\n", s,
+              use_naive ? "naive" : "spine", items.size(), (unsigned long long)hs[2],
+              (unsigned long long)hs[6], e);
     return fl[0] ? SIMBA_BUDGET : 0;
   }
 
@@ -1511,6 +1553,7 @@ class Search final : public SearchSession {
       }
       uint64_t best = ~0ULL;
       int rc = search_size(s, stop, &best, &out->evaluated, &out->device_ms);
+      if (best != ~0ULL && o_.rank_order == 1 && s > 1) best = rtid_rank(ct_.n, s, best);
       out->launches = launches_;
       out->kernel_ms = kernel_ms_;
       out->alg_ops = alg_ops_;
@@ -1720,12 +1763,14 @@ class Batch {
     const int first = o_.size_range ? 1 : 2;
     const int last = o_.size_range ? max_size : max_size - 1;
     for (int i = 0; i < n; ++i) size[i] = first;
-    std::vector<char> active(n, 1);
+    std::vector<char> active(n, 1), inround(n, 0);
+    std::vector<double> swept(n, 0.0);  // candidates of the sizes already searched
     if (first > last)
       for (int i = 0; i < n; ++i) active[i] = 0, (*outs)[i].status = SIMBA_NOT_FOUND;
     auto tabp = [&](int i, int t) {
       return reinterpret_cast<const W*>(d_tab_.as<char>() + tab_off[i] + toff[i][t]);
     };
+    auto next_cost = [&](int i) { return swept[i] + (double)cts_[ct_of[i]].n[size[i]][8]; };
     const size_t smem = ((sizeof(Smem) + 15) & ~size_t(15)) +
                         (((size_t)maxS * maxK * sizeof(W) + 15) / 16 + ((size_t)maxS * sizeof(W) + 15) / 16) * 16;
     SB_CUDA(cudaFuncSetAttribute(spine_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1733,6 +1778,10 @@ class Batch {
     int occ = 1;
     SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, spine_kernel<W>, kThreads, smem));
     const int grid = sms * std::max(occ, 1);
+    SB_CUDA(d_ns_.reserve((size_t)n * 16 + 16));
+    SB_CUDA(cudaMemsetAsync(d_ns_.p, 0, (size_t)n * 16, stream_));
+    std::vector<unsigned long long> ns(2 * (size_t)n + 2);
+    const double growth = round_growth();
     const auto t0 = std::chrono::steady_clock::now();
     SB_CUDA(cudaEventRecord(e0_, stream_));
     stamp_start_kernel<<<1, 1, 0, stream_>>>(d_scal_.as<unsigned long long>() + 3);
@@ -1744,10 +1793,18 @@ class Batch {
     *kernel_ms = 0;
     std::vector<InstDesc<W>> desc(n);
     std::vector<unsigned long long> best(n);
+    std::vector<int> order;
+    unsigned long long start_ns = 0;
     for (;;) {
-      bool any = false;
-      for (int i = 0; i < n; ++i) any |= active[i] != 0;
-      if (!any) break;
+      // Rounds in order of cost: an instance searches its next size in this
+      // round when the candidates it will then have swept are within
+      // `growth` times the cheapest such total, so instances that are cheap
+      // to solve reach their sizes first instead of waiting for every
+      // instance's sweep of each size.
+      double lo = std::numeric_limits<double>::infinity();
+      for (int i = 0; i < n; ++i)
+        if (active[i]) lo = std::min(lo, next_cost(i));
+      if (!(lo < std::numeric_limits<double>::infinity())) break;
       const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
       if (o_.budget_s > 0 && el > o_.budget_s) {
         for (int i = 0; i < n; ++i)
@@ -1758,11 +1815,18 @@ class Batch {
           }
         break;
       }
+      const double theta = lo * growth;
+      order.clear();
+      for (int i = 0; i < n; ++i) {
+        inround[i] = active[i] && next_cost(i) <= theta;
+        if (inround[i]) order.push_back(i);
+      }
+      std::stable_sort(order.begin(), order.end(),
+                       [&](int a, int b) { return next_cost(a) < next_cost(b); });
       ++*rounds;
       // 1. value tables: instances whose current size is tabled build it now
       build_jobs_.clear();
-      for (int i = 0; i < n; ++i) {
-        if (!active[i]) continue;
+      for (int i : order) {
         const int want = std::min(size[i], T[i]);
         const CountTable& ct = cts_[ct_of[i]];
         for (int t = built[i] + 1; t <= want; ++t) {
@@ -1800,15 +1864,24 @@ class Batch {
         ++*launches;
         SB_CUDA(cudaGetLastError());
       }
-      // 2. one task per active instance, pointing at its shared spine list
+      // 2. tasks on the shared spine lists.  Plain: one per instance, the
+      // cheapest first.  Guided: one per (instance, shape-class bucket),
+      // ordered by prior probability per unit of work across all instances
+      // of the round, so the likeliest spines of every instance run first.
       tasks_.clear();
-      orders_.clear();
+      mtasks_.clear();
       const float* priors = o_.class_prior;  // n x 64 in batch mode
       const bool guided = priors != nullptr;
       uint64_t ctx_base = 0, units = 0;
       std::vector<int> naive_insts;
-      for (int i = 0; i < n; ++i) {
-        if (!active[i]) continue;
+      struct Pending {
+        double key;
+        int inst, bucket;
+        unsigned tmpl;
+        uint64_t ctx_base, units;
+      };
+      std::vector<Pending> pend;
+      for (int i : order) {
         const CountTable& ct = cts_[ct_of[i]];
         const int ul = hs_[i].unit_log2 > 0 ? std::min(hs_[i].unit_log2, 40) : 0;
         const ItemTemplate& tp = get_template(ct, std::min(T[i], size[i]), size[i], mask,
@@ -1817,34 +1890,41 @@ class Batch {
           naive_insts.push_back(i);
           continue;
         }
-        if (guided) {  // visit the shape classes by this instance's prior
+        Task mt;
+        memset(&mt, 0, sizeof(mt));
+        mt.ctx_base = ctx_base;
+        mt.inst = (unsigned)i;
+        mt.tmpl = (unsigned)tp.id;
+        mt.bucket = -1;
+        if (tp.nctxs) mtasks_.push_back(mt);
+        if (guided) {
           const float* pr = priors + (size_t)i * 64;
-          int ord[64];
-          float pb[64];
           for (int b = 0; b < 64; ++b) {
-            ord[b] = b;
-            pb[b] = b < 8 ? std::max(pr[b], pr[32 + b]) : pr[b];
+            if (tp.bucket_units[b] == 0) continue;
+            // a unary-chain bucket holds both ~- and neg-rooted chains
+            const double pb = b < 8 ? (double)pr[b] + (double)pr[32 + b] : (double)pr[b];
+            pend.push_back({-(std::max(pb, 1e-12) / (double)tp.bucket_units[b]), i, b,
+                            (unsigned)tp.id, ctx_base, tp.bucket_units[b]});
           }
-          std::stable_sort(ord, ord + 64, [&](int a, int b) { return pb[a] > pb[b]; });
-          TaskOrder to;
-          uint64_t acc = 0;
-          for (int r = 0; r < 64; ++r) {
-            to.order[r] = (unsigned char)ord[r];
-            to.prefix[r] = acc;
-            acc += tp.bucket_units[ord[r]];
-          }
-          to.prefix[64] = acc;
-          orders_.push_back(to);
+        } else {
+          pend.push_back({0.0, i, -1, (unsigned)tp.id, ctx_base, tp.units});
         }
-        Task tk;
-        tk.unit_begin = units;
-        tk.ctx_base = ctx_base;
-        tk.inst = (unsigned)i;
-        tk.tmpl = (unsigned)tp.id;
-        tasks_.push_back(tk);
-        units += tp.units;
         ctx_base += tp.nctxs;
         *alg_ops += tp.alg;
+      }
+      if (guided)
+        std::stable_sort(pend.begin(), pend.end(),
+                         [](const Pending& a, const Pending& b) { return a.key < b.key; });
+      for (const Pending& q : pend) {
+        Task tk;
+        memset(&tk, 0, sizeof(tk));
+        tk.unit_begin = units;
+        tk.ctx_base = q.ctx_base;
+        tk.inst = (unsigned)q.inst;
+        tk.tmpl = q.tmpl;
+        tk.bucket = q.bucket;
+        tasks_.push_back(tk);
+        units += q.units;
       }
       if (tmpl_dirty_) {  // upload the spine lists created since the last round
         SB_CUDA(d_items_.reserve(std::max<size_t>(1, all_items_.size()) * sizeof(Item)));
@@ -1871,6 +1951,7 @@ class Batch {
         d.out = reinterpret_cast<const W*>(d_smp_.as<char>() + out_off[i]);
         d.counts = d_cts_.as<unsigned long long>() + (size_t)ct_of[i] * (kMaxSize + 1) * kCols;
         d.best = d_best_.as<unsigned long long>() + i;
+        d.ns = d_ns_.as<unsigned long long>() + 2 * (size_t)i;
         d.target = (W)hs_[i].out[0];
         d.size = size[i];
         d.S = hs_[i].S;
@@ -1889,12 +1970,11 @@ class Batch {
       p.evaluated = sc + 2;
       p.start_ns = sc + 3;
       p.flags = reinterpret_cast<int*>(sc + 4);
+      p.hits = sc + 6;
       p.maxS = maxS;
       p.maxK = maxK;
-      p.stop_on_match = 1;
+      p.stop_on_match = guided ? 2 : 1;  // guided: any verified match of the size
       p.budget_ns = o_.budget_s > 0 ? (unsigned long long)(o_.budget_s * 1e9) : 0;
-      cudaEvent_t k0 = e1_;
-      (void)k0;
       float kms = 0;
       cudaEvent_t ka, kb;
       SB_CUDA(cudaEventCreate(&ka));
@@ -1906,25 +1986,24 @@ class Batch {
                                 cudaMemcpyHostToDevice, stream_));
         p.tasks = d_tasks_.as<Task>();
         p.ntasks = (int)tasks_.size();
-        if (guided) {
-          SB_CUDA(d_orders_.reserve(orders_.size() * sizeof(TaskOrder)));
-          SB_CUDA(cudaMemcpyAsync(d_orders_.p, orders_.data(), orders_.size() * sizeof(TaskOrder),
-                                  cudaMemcpyHostToDevice, stream_));
-          p.orders = d_orders_.as<TaskOrder>();
-          p.buckets = d_buckets_.as<TmplBuckets>();
-          p.stop_on_match = 2;  // any verified match of the size
-        }
+        p.buckets = d_buckets_.as<TmplBuckets>();
         p.tmpls = d_tdesc_.as<TmplDesc>();
         p.items = d_items_.as<Item>();
         p.nitems = (int)all_items_.size();
         p.total_units = units;
-        if (ctx_base) {
+        if (ctx_base) {  // contexts of the fused spines, one task per instance
           SB_CUDA(d_ctx_.reserve(ctx_base * sizeof(Ctx<W>)));
+          SB_CUDA(d_mtasks_.reserve(mtasks_.size() * sizeof(Task)));
+          SB_CUDA(cudaMemcpyAsync(d_mtasks_.p, mtasks_.data(), mtasks_.size() * sizeof(Task),
+                                  cudaMemcpyHostToDevice, stream_));
           p.sitems = d_small_.as<Item>();
           p.nsitems = (int)all_small_.size();
           p.nctxs = ctx_base;
+          Params<W> m = p;
+          m.tasks = d_mtasks_.as<Task>();
+          m.ntasks = (int)mtasks_.size();
           const int mb = (int)std::min<uint64_t>((ctx_base + 255) / 256, (uint64_t)sms * 8);
-          materialize_kernel<W><<<mb, 256, 0, stream_>>>(p, d_ctx_.as<Ctx<W>>());
+          materialize_kernel<W><<<mb, 256, 0, stream_>>>(m, d_ctx_.as<Ctx<W>>());
           ++*launches;
           p.ctxs = d_ctx_.as<Ctx<W>>();
         }
@@ -1943,6 +2022,7 @@ class Batch {
       }
       SB_CUDA(cudaEventRecord(kb, stream_));
       SB_CUDA(cudaMemcpyAsync(best.data(), d_best_.p, (size_t)n * 8, cudaMemcpyDeviceToHost, stream_));
+      SB_CUDA(cudaMemcpyAsync(ns.data(), d_ns_.p, (size_t)n * 16, cudaMemcpyDeviceToHost, stream_));
       unsigned long long hs[8];
       SB_CUDA(cudaMemcpyAsync(hs, d_scal_.p, sizeof(hs), cudaMemcpyDeviceToHost, stream_));
       SB_CUDA(cudaStreamSynchronize(stream_));
@@ -1951,6 +2031,7 @@ class Batch {
       cudaEventDestroy(kb);
       *kernel_ms += kms;
       *evaluated += hs[2];
+      start_ns = hs[3];
       const int* fl = reinterpret_cast<const int*>(hs + 4);
       if (fl[1]) {
         set_last_error("inversion failed on a level marked invertible");
@@ -1958,8 +2039,7 @@ class Batch {
       }
       const double now = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
       // 4. retire solved instances, advance the others
-      for (int i = 0; i < n; ++i) {
-        if (!active[i]) continue;
+      for (int i : order) {
         Out& r = (*outs)[i];
         const CountTable& ct = cts_[ct_of[i]];
         const int s = size[i];
@@ -1978,7 +2058,11 @@ class Batch {
           r.op = op;
           r.rank = best[i];
           r.status = host_check(r.postfix, hs_[i]) ? SIMBA_OK : SIMBA_E_INTERNAL;
-          r.seconds = now;
+          // device time of the solution: the first verified match (guided:
+          // the search stops there), or the last unit of the instance that
+          // ran (plain: every rank below the answer is then searched)
+          const unsigned long long t = guided ? ns[2 * i] : std::max(ns[2 * i], ns[2 * i + 1]);
+          r.seconds = t > start_ns ? (double)(t - start_ns) * 1e-9 : now;
           active[i] = 0;
         } else if (fl[0]) {
           r.status = SIMBA_BUDGET;
@@ -1986,12 +2070,28 @@ class Batch {
           active[i] = 0;
         } else {
           r.candidates += ct.n[s][8];
+          swept[i] += (double)ct.n[s][8];
           if (++size[i] > last) {
             r.status = SIMBA_NOT_FOUND;
             r.seconds = now;
             active[i] = 0;
           }
         }
+      }
+      if (o_.verbose) {
+        int solved = 0, smin = kMaxSize, smax = 0;
+        for (int i : order) {
+          solved += best[i] != ~0ULL;
+          smin = std::min(smin, size[i] - (best[i] == ~0ULL ? 1 : 0));
+          smax = std::max(smax, size[i] - (best[i] == ~0ULL ? 1 : 0));
+        }
+        fprintf(stderr,
+                "round %3d | t %8.3f s | insts %6zu (sizes %d-%d) | tasks %7zu | units %10llu | "
+                "ctxs %10llu | naive %4zu | evaluated %.3e | hits %.3e | kernels %9.3f ms | "
+                "solved %5d%s\n",
+                *rounds, now, order.size(), smin, smax, tasks_.size(), (unsigned long long)units,
+                (unsigned long long)ctx_base, naive_insts.size(), (double)hs[2], (double)hs[6], kms,
+                solved, fl[0] ? " | budget" : "");
       }
     }
     SB_CUDA(cudaEventRecord(e1_, stream_));
@@ -2004,6 +2104,16 @@ class Batch {
   }
 
  private:
+  // Width of a cost-ordered round: instances whose swept total after their
+  // next size is within this factor of the cheapest one run in the round
+  // (SIMBA_ROUND_GROWTH overrides; 0 or less means every active instance,
+  // i.e. all instances step through the sizes together).
+  static double round_growth() {
+    const char* e = getenv("SIMBA_ROUND_GROWTH");
+    const double g = e ? atof(e) : 64.0;
+    return g > 0 ? std::max(g, 1.0) : std::numeric_limits<double>::infinity();
+  }
+
   // Bucket of a spine in a guided list: its (primary) shape class.
   static int bucket_of(const Item& it, int s) {
     int a, b;
@@ -2116,12 +2226,12 @@ class Batch {
   std::vector<Item> all_items_, all_small_;  // every spine list, concatenated
   std::vector<TmplDesc> tdescs_;
   std::vector<TmplBuckets> all_buckets_;
-  std::vector<TaskOrder> orders_;
+  std::vector<Task> mtasks_;  // one per instance with fused spines (materialisation)
   bool tmpl_dirty_ = false;
   std::vector<Task> tasks_;
   std::vector<BuildJob<W>> build_jobs_;
   DevBuf d_tab_, d_smp_, d_cts_, d_best_, d_desc_, d_scal_, d_items_, d_small_, d_ctx_, d_jobs_,
-      d_tasks_, d_tdesc_, d_buckets_, d_orders_;
+      d_tasks_, d_tdesc_, d_buckets_, d_mtasks_, d_ns_;
 };
 
 template <class W>

@@ -30,6 +30,7 @@
 #include <chrono>
 #include <climits>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -123,6 +124,41 @@ __device__ int hash_insert(unsigned long long* keys, unsigned* vals, unsigned lo
   return INS_FULL;
 }
 
+// Keep / store one composed candidate (x, y) whose fingerprint is (A, B):
+// insert into the hash set, append the vector when it is kept, compare it
+// with the target.  `elem(i)` recomputes element i of the vector.
+template <class W, int OP, class Elem>
+__device__ __forceinline__ void vfb_offer(const VfbArgs<W>& a, unsigned long long x, unsigned long long y,
+                                          unsigned long long A, unsigned B, Elem elem) {
+  const int ins = hash_insert(a.keys, a.vals, a.mask, A, B);
+  bool keep;
+  if (a.inverted) keep = ins != INS_NEW;  // INS_FULL is kept too, as in the reference
+  else {
+    if (ins == INS_FULL) atomicOr(&a.flags[1], 1);
+    keep = ins == INS_NEW;
+  }
+  if (!keep) return;
+  const unsigned long long row = atomicAdd(a.nrows, 1ULL);
+  bool match = true;
+  W* out = row < a.cap ? a.rows + row * a.S : nullptr;
+  for (int i = 0; i < a.S; ++i) {
+    const W v = elem(i);
+    match &= v == a.target[i];
+    if (out) out[i] = v;
+  }
+  if (out) {
+    a.rop[row] = (int8_t)OP;
+    a.rl[row] = (uint32_t)x;
+    a.rr[row] = (uint32_t)y;
+  } else {
+    atomicOr(&a.flags[0], 1);
+  }
+  if (match) {
+    atomicCAS(a.found, ~0ULL, (x << 32) | y);
+    atomicMin(a.found_launch, a.launch);
+  }
+}
+
 template <class W, int OP>
 __global__ void __launch_bounds__(256) vfb_compose_kernel(VfbArgs<W> a) {
   if (*(volatile int*)a.found_launch < a.launch) return;  // an earlier block found it
@@ -154,34 +190,57 @@ __global__ void __launch_bounds__(256) vfb_compose_kernel(VfbArgs<W> a) {
       const W v = vop<W, OP>(L[i], unary ? W(0) : R[i]);
       fp_step(fa, fb, (unsigned long long)v, i);
     }
-    const unsigned long long A = fp_final(fa, S);
-    const unsigned B = fp_check(fb);
-    const int ins = hash_insert(a.keys, a.vals, a.mask, A, B);
-    bool keep;
-    if (a.inverted) keep = ins != INS_NEW;  // INS_FULL is kept too, as in the reference
-    else {
-      if (ins == INS_FULL) atomicOr(&a.flags[1], 1);
-      keep = ins == INS_NEW;
-    }
-    if (!keep) continue;
-    const unsigned long long row = atomicAdd(a.nrows, 1ULL);
-    bool match = true;
-    W* out = row < a.cap ? a.rows + row * S : nullptr;
-    for (int i = 0; i < S; ++i) {
-      const W v = vop<W, OP>(L[i], unary ? W(0) : R[i]);
-      match &= v == a.target[i];
-      if (out) out[i] = v;
-    }
-    if (out) {
-      a.rop[row] = (int8_t)OP;
-      a.rl[row] = (uint32_t)x;
-      a.rr[row] = (uint32_t)y;
-    } else {
-      atomicOr(&a.flags[0], 1);
-    }
-    if (match) {
-      atomicCAS(a.found, ~0ULL, (x << 32) | y);
-      atomicMin(a.found_launch, a.launch);
+    vfb_offer<W, OP>(a, x, y, fp_final(fa, S), fp_check(fb),
+                     [&](int i) { return vop<W, OP>(L[i], unary ? W(0) : R[i]); });
+  }
+}
+
+// Binary compositions, tiled: a CTA stages kTL left rows and kTR right rows
+// in shared memory (row pitch S+1 words, so the 32 right rows a warp reads
+// fall in different banks) and composes all kTL x kTR pairs from there, so
+// each operand row crosses L2/HBM once per tile instead of once per pair.
+// Thread t takes right row t % kTR and left rows t / kTR + 8 j, j < 2.
+constexpr int kTL = 16, kTR = 32;
+
+template <class W, int OP>
+__global__ void __launch_bounds__(256) vfb_tile_kernel(VfbArgs<W> a) {
+  if (*(volatile int*)a.found_launch < a.launch) return;  // an earlier block found it
+  extern __shared__ __align__(16) unsigned char vfb_smem[];
+  W* sl = reinterpret_cast<W*>(vfb_smem);
+  const int S = a.S, P = S + 1;
+  W* sr = sl + kTL * P;
+  const unsigned long long tl = (a.nl + kTL - 1) / kTL, tr = (a.nr + kTR - 1) / kTR;
+  const int ri = threadIdx.x % kTR, li0 = threadIdx.x / kTR;
+  for (unsigned long long tile = blockIdx.x; tile < tl * tr; tile += gridDim.x) {
+    const unsigned long long lb = (tile / tr) * kTL, rb = (tile % tr) * kTR;
+    const int nl = (int)(a.nl - lb < (unsigned long long)kTL ? a.nl - lb : kTL);
+    const int nr = (int)(a.nr - rb < (unsigned long long)kTR ? a.nr - rb : kTR);
+    __syncthreads();  // the previous tile's reads are done
+    const W* gl = a.rows + (a.l0 + lb) * S;
+    const W* gr = a.rows + (a.r0 + rb) * S;
+    for (int q = threadIdx.x; q < nl * S; q += blockDim.x) sl[(q / S) * P + q % S] = gl[q];
+    for (int q = threadIdx.x; q < nr * S; q += blockDim.x) sr[(q / S) * P + q % S] = gr[q];
+    __syncthreads();
+    if (ri >= nr) continue;
+    const W* R = sr + ri * P;
+    const unsigned long long y = a.r0 + rb + ri;
+#pragma unroll
+    for (int j = 0; j < kTL / 8; ++j) {
+      const int li = li0 + 8 * j;
+      if (li >= nl) break;
+      const W* L = sl + li * P;
+      const unsigned long long x = a.l0 + lb + li;
+      unsigned long long fa = 0x243F6A8885A308D3ULL, fb = 0, ga = fa, gb = 0;
+      for (int i = 0; i < S; ++i) {
+        const W l = L[i], r = R[i];
+        fp_step(fa, fb, (unsigned long long)vop<W, OP>(l, r), i);
+        if (a.swap) fp_step(ga, gb, (unsigned long long)vop<W, OP>(r, l), i);
+      }
+      vfb_offer<W, OP>(a, x, y, fp_final(fa, S), fp_check(fb),
+                       [&](int i) { return vop<W, OP>(L[i], R[i]); });
+      if (a.swap)
+        vfb_offer<W, OP>(a, y, x, fp_final(ga, S), fp_check(gb),
+                         [&](int i) { return vop<W, OP>(R[i], L[i]); });
     }
   }
 }
@@ -197,6 +256,37 @@ __global__ void vfb_init_kernel(VfbArgs<W> a, int k) {
   a.rop[j] = -1;
   a.rl[j] = (uint32_t)j;
   a.rr[j] = 0;
+}
+
+template <class W>
+static void launch_tiled(int op, int grid, size_t smem, cudaStream_t st, const VfbArgs<W>& a) {
+  switch (op) {
+    case OP_AND: vfb_tile_kernel<W, OP_AND><<<grid, 256, smem, st>>>(a); break;
+    case OP_OR: vfb_tile_kernel<W, OP_OR><<<grid, 256, smem, st>>>(a); break;
+    case OP_XOR: vfb_tile_kernel<W, OP_XOR><<<grid, 256, smem, st>>>(a); break;
+    case OP_ADD: vfb_tile_kernel<W, OP_ADD><<<grid, 256, smem, st>>>(a); break;
+    case OP_SUB: vfb_tile_kernel<W, OP_SUB><<<grid, 256, smem, st>>>(a); break;
+    default: vfb_tile_kernel<W, OP_MUL><<<grid, 256, smem, st>>>(a); break;
+  }
+}
+
+template <class W>
+static int tile_smem_setup(int S, size_t* smem) {
+  *smem = (size_t)(kTL + kTR) * (S + 1) * sizeof(W);
+  const int ops[6] = {OP_AND, OP_OR, OP_XOR, OP_ADD, OP_SUB, OP_MUL};
+  for (int op : ops) {
+    const void* f = nullptr;
+    switch (op) {
+      case OP_AND: f = (const void*)vfb_tile_kernel<W, OP_AND>; break;
+      case OP_OR: f = (const void*)vfb_tile_kernel<W, OP_OR>; break;
+      case OP_XOR: f = (const void*)vfb_tile_kernel<W, OP_XOR>; break;
+      case OP_ADD: f = (const void*)vfb_tile_kernel<W, OP_ADD>; break;
+      case OP_SUB: f = (const void*)vfb_tile_kernel<W, OP_SUB>; break;
+      default: f = (const void*)vfb_tile_kernel<W, OP_MUL>; break;
+    }
+    SB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
+  }
+  return 0;
 }
 
 template <class W>
@@ -319,6 +409,18 @@ static int vfb_typed(const HostInstance& h, int max_len, const EngineOptions& o,
   start[2] = (unsigned long long)k;
   out->rows_per_size[1] = k;
   const int grid = sms * 8;
+  // tiled binary compositions unless SIMBA_VFB_TILED=0 (the per-pair kernel)
+  const char* te = getenv("SIMBA_VFB_TILED");
+  const bool tiled = !(te && te[0] == '0');
+  size_t tile_smem = 0;
+  int tile_grid = grid;
+  if (tiled) {
+    if (tile_smem_setup<W>(S, &tile_smem)) return SIMBA_E_CUDA;
+    int occ = 1;
+    SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, vfb_tile_kernel<W, OP_MUL>, 256,
+                                                          tile_smem));
+    tile_grid = sms * std::max(occ, 1);
+  }
   int launch = 0;
   struct LaunchInfo {
     int op;
@@ -358,7 +460,11 @@ static int vfb_typed(const HostInstance& h, int max_len, const EngineOptions& o,
           if (n == 0) continue;
           a.launch = launch++;
           info.push_back({op, n});
-          launch_compose<W>(op, (int)std::min<unsigned long long>((n + 255) / 256, grid), st, a);
+          const unsigned long long tiles = ((a.nl + kTL - 1) / kTL) * ((a.nr + kTR - 1) / kTR);
+          if (tiled)
+            launch_tiled<W>(op, (int)std::min<unsigned long long>(tiles, tile_grid), tile_smem, st, a);
+          else
+            launch_compose<W>(op, (int)std::min<unsigned long long>((n + 255) / 256, grid), st, a);
         }
       }
     }

@@ -7,7 +7,9 @@ and the reference VFB executable (``oracle/_ref/vfb_full_cache``,
 vfb/src/full-cache.cu:776-854) and records the CSV line each one prints.
 It also times unsatisfiable sweeps, which give the reference's
 candidate-evals/s.  Output: one JSON file (path = first argument) that is
-committed as ``tests/golden/ref_results_u32.json``.
+committed as ``tests/golden/ref_results_u32.json``; with ``--rtid`` after
+the path, the reference's RTid build alone (``oracle/_ref/simba_rtid``),
+committed as ``tests/golden/ref_results_rtid_u32.json``.
 """
 import json
 import subprocess
@@ -23,6 +25,7 @@ sys.path.insert(0, str(ROOT))
 from simba_b200.instances import make_instance  # noqa: E402
 
 SIMBA = ROOT / "oracle" / "_ref" / "simba_nocache"
+SIMBA_RTID = ROOT / "oracle" / "_ref" / "simba_rtid"
 VFB = ROOT / "oracle" / "_ref" / "vfb_full_cache"
 
 
@@ -40,6 +43,23 @@ def run(exe: Path, path: Path, max_len: int, timeout: float) -> dict:
                 "wall": wall, "stderr_tail": p.stderr[-400:]}
     except subprocess.TimeoutExpired:
         return {"rc": None, "timeout": timeout, "wall": time.perf_counter() - t0}
+
+
+def main_rtid(out_path: str) -> None:
+    """The reference's RTid build (simba/src/nocache_rtid.cu) on every golden
+    instance; committed as tests/golden/ref_results_rtid_u32.json."""
+    insts = json.loads((HERE / "ref_instances_u32.json").read_text())
+    res = {"simba_rtid": []}
+    with tempfile.TemporaryDirectory() as td:
+        td = Path(td)
+        for idx, d in enumerate(insts):
+            p = td / f"inst_{idx}.json"
+            p.write_text(json.dumps(d))
+            ml = d["gen_size"] + 1
+            r = run(SIMBA_RTID, p, ml, 60)
+            r.update({"idx": idx, "max_len": ml})
+            res["simba_rtid"].append(r)
+    Path(out_path).write_text(json.dumps(res, indent=1))
 
 
 def main(out_path: str) -> None:
@@ -72,4 +92,7 @@ def main(out_path: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1])
+    if len(sys.argv) > 2 and sys.argv[2] == "--rtid":
+        main_rtid(sys.argv[1])
+    else:
+        main(sys.argv[1])

@@ -99,3 +99,20 @@ def test_solve_rejects_bad_limits():
     big.inputs = np.zeros((8, 17), dtype=np.uint64)
     with pytest.raises(S.SimbaError):
         S.solve(big, 5)
+
+
+def test_rtid_option_is_rejected_where_unsupported():
+    """RTid order is a single-instance option: batch, sessions, the static
+    entry point and guided / naive searches refuse it before any GPU work."""
+    import numpy as np
+    import simba_b200 as S
+    from simba_b200.instances import make_instance
+    inst = make_instance(5, 2, 16, 1, word_bits=64)
+    prior = np.ones(64, dtype=np.float32)
+    for call in (lambda: S.solve_batch([inst], 8, rtid=True),
+                 lambda: S.solve_noalloc(inst, 8, rtid=True),
+                 lambda: S.Session(inst, rtid=True),
+                 lambda: S.solve(inst, 8, rtid=True, naive=True),
+                 lambda: S.solve(inst, 8, rtid=True, class_prior=prior)):
+        with pytest.raises(S.SimbaError, match="rank_order|RTid"):
+            call()

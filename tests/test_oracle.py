@@ -158,3 +158,71 @@ def test_scan_range_counts(oracle):
     inst = make_instance(9, 2, 32, 3, word_bits=64, unsat=True)
     e, mr, nh = oracle.scan_range(inst.inputs, inst.outputs, 6, 0, 5000, 64)
     assert e == 5000 and nh == 0 and mr == 2 ** 64 - 1
+
+
+def _rtid_brute(oracle, inst, size, op, bits, reference_map):
+    """Smallest thread position t of block (size, op) whose rank matches."""
+    t = oracle.count_table(size, inst.num_variables)
+    off = int(sum(int(x) for x in t[size][:op]))
+    N = int(t[size][op])
+    c = oracle.rtid_multiplier(N)
+    T = (N + 1023) // 1024 * 1024 if reference_map else N
+    for x in range(T):
+        r = off + ((x * 2246822507) % (1 << 64)) % N if reference_map else off + (x * c) % N
+        if oracle.check(oracle.unrank(r, size, t), inst.inputs, inst.outputs, bits):
+            return r
+    return None
+
+
+@pytest.mark.parametrize("reference_map", [False, True])
+def test_rtid_order_brute_force(oracle, reference_map):
+    """RTid order: the first operator block with a match (the same block as
+    the rank order when every rank is visited) and, inside it, the match of
+    the smallest thread position, checked by a plain loop."""
+    for seed in range(8):
+        inst = make_instance(6 + seed % 3, 1 + seed % 3, 16, 700 + seed, word_bits=64)
+        a = oracle.search(inst.inputs, inst.outputs, 10, 64)
+        b = oracle.search_rtid(inst.inputs, inst.outputs, 10, 64, reference_map=reference_map)
+        assert a["found"] == b["found"]
+        if not a["found"]:
+            continue
+        assert (a["size"], a["op"], a["candidates"]) == (b["size"], b["op"], b["candidates"])
+        assert oracle.check(b["postfix"], inst.inputs, inst.outputs, 64)
+        assert b["rank"] == _rtid_brute(oracle, inst, b["size"], b["op"], 64, reference_map)
+
+
+def test_rtid_multiplier_is_coprime(oracle):
+    import math
+    C = 2246822507
+    assert oracle.rtid_multiplier(1000) == C
+    for n in (15809, 142123 * 7, 15809 * 142123, 2 * 15809 * 3):
+        c = oracle.rtid_multiplier(n)
+        assert c > C and math.gcd(c, n) == 1
+        assert all(math.gcd(x, n) != 1 for x in range(C, c))
+    # the reference's map on such a block visits only multiples of the gcd
+    n = 15809 * 4
+    assert len({(x * C) % n for x in range((n + 1023) // 1024 * 1024)}) == 4
+
+
+def test_oracle_rtid_matches_reference_rtid(oracle):
+    """The reference's simba_rtid executable on the golden instances: same
+    size and operator block; the returned expression is a match."""
+    import json
+    from pathlib import Path
+    g = Path(__file__).resolve().parent / "golden"
+    f = g / "ref_results_rtid_u32.json"
+    if not f.exists():
+        pytest.skip("reference RTid results not generated")
+    insts = json.loads((g / "ref_instances_u32.json").read_text())
+    same = 0
+    for r in json.loads(f.read_text())["simba_rtid"]:
+        inst = Instance.from_json(insts[r["idx"]])
+        o = oracle.search_rtid(inst.inputs, inst.outputs, r["max_len"], 32, reference_map=True)
+        if r["expr"] == "Not found !":
+            assert not o["found"]
+            continue
+        p = infix_to_postfix(r["expr"])
+        assert oracle.check(p, inst.inputs, inst.outputs, 32)
+        assert o["found"] and len(p) == o["size"] and OPS.index(p[-1]) == o["op"]
+        same += p == o["postfix"]
+    assert same >= 100

@@ -175,3 +175,63 @@ def test_shards_of_a_size_combine_to_the_full_search(oracle):
                 if whole["best_rank"] is not None:
                     break  # units above a match may be skipped differently
                 assert sum(p["evaluated"] for p in parts) == whole["evaluated"]
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_rtid_order_matches_oracle(oracle, bits):
+    """RTid order (simba_rtid): same size, block, candidate count and the same
+    expression (the match of the smallest thread position) as the oracle."""
+    for seed in range(12):
+        inst = make_instance(5 + seed % 6, 1 + seed % 3, (16, 32, 64)[seed % 3], 5100 + seed,
+                             word_bits=bits)
+        r = S.solve(inst, 12, rtid=True)
+        o = oracle.search_rtid(inst.inputs, inst.outputs, 12, bits)
+        assert r.found == o["found"]
+        assert r.candidates == o["candidates"]
+        if o["found"]:
+            assert (r.size, r.op, r.rank, r.postfix) == (o["size"], o["op"], o["rank"], o["postfix"])
+
+
+def test_rtid_large_blocks_and_deep_spines(oracle):
+    """Blocks of ~1e9 ranks (64-bit products in the position map) and small
+    tables (explicit levels, fused spines): still the oracle's answer."""
+    for seed in range(3):
+        inst = make_instance(11, 3, 32, 5300 + seed, word_bits=64)
+        for tb in (0, 1 << 16):
+            r = S.solve(inst, 12, rtid=True, table_bytes=tb)
+            o = oracle.search_rtid(inst.inputs, inst.outputs, 12, 64)
+            assert (r.found, r.size, r.op, r.rank) == (o["found"], o["size"], o["op"], o["rank"])
+
+
+def test_rtid_cli_dropin(tmp_path, oracle, golden):
+    exe = ROOT / "simba_b200" / "bin" / "simba_rtid"
+    for r in golden["results"]["simba"][:10]:
+        d = golden["instances"][r["idx"]]
+        p = tmp_path / f"inst_{r['idx']}.json"
+        p.write_text(json.dumps(d))
+        out = subprocess.run([str(exe), str(p), str(r["max_len"])], capture_output=True,
+                             text=True, timeout=120)
+        assert out.returncode == 0
+        path, expr, secs = out.stdout.strip().rsplit(",", 2)
+        inst = Instance.from_json(d)
+        o = oracle.search_rtid(inst.inputs, inst.outputs, r["max_len"], 32)
+        assert expr == (S.format_postfix(o["postfix"]) if o["found"] else "Not found !")
+
+
+def test_rtid_matches_reference_rtid_executable(oracle):
+    """The reference's simba_rtid on the golden instances: same size and
+    operator block, and a verified match."""
+    g = ROOT / "tests" / "golden"
+    f = g / "ref_results_rtid_u32.json"
+    if not f.exists():
+        pytest.skip("reference RTid results not generated")
+    insts = json.loads((g / "ref_instances_u32.json").read_text())
+    for r in json.loads(f.read_text())["simba_rtid"]:
+        inst = Instance.from_json(insts[r["idx"]])
+        res = S.solve(inst, r["max_len"], rtid=True)
+        if r["expr"] == "Not found !":
+            assert not res.found
+            continue
+        p = infix_to_postfix(r["expr"])
+        assert res.found and res.size == len(p) and res.postfix[-1] == p[-1]
+        assert oracle.check(res.postfix, inst.inputs, inst.outputs, 32)
