@@ -55,7 +55,10 @@ typedef struct {
   int32_t verbose;       /* progress lines on stderr                             */
   int32_t engine;        /* 0: tabled spine engine; 1: one thread per rank       */
   double budget_seconds; /* 0 = unlimited                                        */
-  int64_t table_bytes;   /* cap on the value tables, 0 = default (4 GiB)         */
+  int64_t table_bytes;   /* cap on the value tables, 0 = default (8 GiB); the
+                            tables are kept for sample 0 and, as match
+                            filters, for samples 1..3 (instances with fewer
+                            samples keep fewer), all inside this cap         */
   uint64_t stream;       /* cudaStream_t to launch on (0 = library-owned stream)  */
   int64_t vfb_cache_rows;/* VFB row capacity, 0 = the reference's rule
                             (max pitch / (4 * samples), full-cache.cu:713-718)  */
@@ -187,12 +190,14 @@ typedef struct {
  * candidates it will then have swept are within 64x (environment
  * SIMBA_ROUND_GROWTH; 0 = every active instance) of the cheapest active
  * instance's, and the round's queue runs the cheapest instances first.
- * opt->table_bytes caps each instance's value tables (0 = 8 MiB);
+ * opt->table_bytes caps each instance's value tables, filter samples
+ * included (0 = 8 MiB);
  * opt->budget_seconds bounds the whole batch.  With opt->class_prior set it
  * points to n x 64 priors (one row per instance, e.g. from
  * simba_mlp_predict) and the batch is guided: the queue holds one entry per
- * (instance, shape class), ordered by prior per unit of work across the
- * round, and an instance retires at its first verified match. */
+ * (instance, shape class), instances cheapest first and each instance's
+ * classes by prior per unit of work, and an instance retires at its first
+ * verified match. */
 int simba_solve_batch(const simba_instance *insts, int n, int max_size, const simba_options *opt,
                       simba_batch_result *results, simba_batch_stats *stats);
 
@@ -271,6 +276,9 @@ int simba_mlp_train_step(simba_mlp *mlp, const simba_instance *insts, int n, con
 /* Gradients of the mean cross-entropy (param_count floats), no update. */
 int simba_mlp_gradients(simba_mlp *mlp, const simba_instance *insts, int n, const int32_t *labels,
                         float *grads, float *loss);
+/* One Adam step with the given gradients (param_count floats): data-parallel
+ * training applies the ranks' all-reduced mean gradient on every rank. */
+int simba_mlp_apply(simba_mlp *mlp, const float *grads, float lr);
 /* Class probabilities, n x 64. */
 int simba_mlp_predict(simba_mlp *mlp, const simba_instance *insts, int n, float *probs);
 /* The features the network reads, n x 8192 (values -1, 0, +1). */

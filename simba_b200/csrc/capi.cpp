@@ -627,6 +627,11 @@ int simba_mlp_gradients(simba_mlp* mlp, const simba_instance* insts, int n, cons
   return mlp_gradients(mlp->m, hs, labels, grads, loss);
 }
 
+int simba_mlp_apply(simba_mlp* mlp, const float* grads, float lr) {
+  if (!mlp || !grads) return SIMBA_E_ARG;
+  return mlp_apply(mlp->m, grads, lr);
+}
+
 int simba_mlp_predict(simba_mlp* mlp, const simba_instance* insts, int n, float* probs) {
   if (!mlp || !probs) return SIMBA_E_ARG;
   std::vector<HostInstance> hs;

@@ -116,6 +116,7 @@ void mlp_destroy(Mlp* m);
 int mlp_train_step(Mlp* m, const std::vector<HostInstance>& hs, const int* labels, float lr, float* loss);
 int mlp_gradients(Mlp* m, const std::vector<HostInstance>& hs, const int* labels, float* grads,
                   float* loss);
+int mlp_apply(Mlp* m, const float* grads, float lr);
 int mlp_predict(Mlp* m, const std::vector<HostInstance>& hs, float* probs);
 int mlp_features(Mlp* m, const std::vector<HostInstance>& hs, float* out);
 int mlp_get_params(Mlp* m, float* h);

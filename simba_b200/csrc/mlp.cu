@@ -398,6 +398,20 @@ class Mlp {
     return 0;
   }
 
+  // One Adam step with gradients computed elsewhere (data-parallel training:
+  // the ranks' gradients, averaged by an all-reduce).
+  int apply(const float* grads, float lr) {
+    SB_CUDA(cudaMemcpyAsync(g_.p, grads, mlp_param_count() * 4, cudaMemcpyHostToDevice, st_));
+    ++step_;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, (float)step_), c2 = 1.f - std::pow(b2, (float)step_);
+    adam_kernel<<<2048, 256, 0, st_>>>(w_.as<float>(), g_.as<float>(), m_.as<float>(), v_.as<float>(),
+                                       wb_.as<bf16>(), mlp_param_count(), lr, b1, b2, 1e-8f, c1, c2);
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaStreamSynchronize(st_));
+    return 0;
+  }
+
   int gradients(const std::vector<HostInstance>& hs, const int* labels, float* grads, float* loss) {
     int rc = features(hs, &X_);
     if (rc) return rc;
@@ -455,6 +469,7 @@ int mlp_gradients(Mlp* m, const std::vector<HostInstance>& hs, const int* labels
                   float* loss) {
   return m->gradients(hs, labels, grads, loss);
 }
+int mlp_apply(Mlp* m, const float* grads, float lr) { return m->apply(grads, lr); }
 int mlp_predict(Mlp* m, const std::vector<HostInstance>& hs, float* probs) { return m->predict(hs, probs); }
 int mlp_features(Mlp* m, const std::vector<HostInstance>& hs, float* out) { return m->features_host(hs, out); }
 int mlp_get_params(Mlp* m, float* h) { return m->get_params(h); }

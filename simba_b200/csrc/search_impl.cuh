@@ -57,14 +57,13 @@ namespace simba {
 
 constexpr int kMaxDepth = 12;  // spine levels
 constexpr int kThreads = 256;  // CTA size of the search kernels
-constexpr int kQueue = 128;    // shared-memory queue of sample-0 matches
-// Tuning knobs (compile-time): contexts per thread, software pipelining of
-// the bottom-value loads, minimum resident CTAs per SM.
+constexpr int kQueue = 128;    // shared-memory queue of matches to verify
+constexpr int kPre = 256;      // shared-memory queue of sample-0 matches to filter
+constexpr int kPreG = 262144;  // the same queue per CTA in global memory, when given
+// Tuning knobs (compile-time): contexts per thread, minimum resident CTAs
+// per SM.
 #ifndef SIMBA_KR
 #define SIMBA_KR 8
-#endif
-#ifndef SIMBA_PIPE
-#define SIMBA_PIPE 0
 #endif
 #ifndef SIMBA_MINB
 #define SIMBA_MINB 0
@@ -76,6 +75,7 @@ constexpr int kQueue = 128;    // shared-memory queue of sample-0 matches
 #endif
 constexpr int kR = SIMBA_KR;   // contexts per thread
 constexpr int kMaxExplicit = 2;
+constexpr int kExtra = 3;       // samples besides sample 0 with value tables (match filters)
 
 // One level of a spine, top-down (level 0 is the root).
 struct Level {
@@ -104,7 +104,7 @@ struct alignas(16) Item {
   uint16_t G, L;        // G context groups x L value lanes = kThreads
   int8_t depth, inv, bottom, full, nexp;
   int8_t fused;         // 1: contexts are read from the materialised list
-  int8_t pad[2];
+  uint16_t cpu;         // context blocks per work unit (> 1 for small bottoms)
   uint64_t ctx_off;     // fused: first context in Params::ctxs
   uint32_t inst;        // instance (index into Params::insts)
   float prio;           // guided search: prior of the spine's shape class
@@ -112,13 +112,22 @@ struct alignas(16) Item {
 };
 
 // A materialised context of a fused group: the bottom-value constraint
-// (v & M) == K and the rank of candidate v = base + v * coefv.
+// (v & M) == K, the rank base of candidate v (base + v * the member spine's
+// coefv), and where the context comes from (for the sample-1 filter).
 template <class W>
 struct Ctx {
   W M, K;
-  unsigned long long base, coefv;
+  unsigned long long base;
+  unsigned member;  // index of the member spine in Params::sitems
+  unsigned c;       // context index inside that spine
 };
 static_assert(sizeof(Item) % 16 == 0, "Item must be 16-byte sized");
+
+// Work units of a spine: groups of `cpu` context blocks x value blocks.
+SB_HD uint64_t item_units(const Item& it) {
+  const uint64_t cpu = it.cpu ? it.cpu : 1;
+  return (it.cblocks + cpu - 1) / cpu * it.vblocks;
+}
 
 // Everything the kernels need about one instance (several per launch in
 // batch mode): value tables, samples, count table, the sample-0 target, the
@@ -132,7 +141,9 @@ struct alignas(16) InstDesc {
   unsigned long long* best;         // minimum verified matching rank
   unsigned long long* ns;           // batch, or null: [0] first verified match,
                                     // [1] last unit that ran (globaltimer ns)
+  const W* tabx[kExtra][kMaxSize + 1];  // value tables on samples 1..kExtra (null: absent)
   W target;                         // output on sample 0
+  W targetx[kExtra];                // outputs on samples 1..kExtra
   int size;
   int S, K;
   int rtid;                         // 1: best holds RTid keys (positions), not ranks
@@ -185,6 +196,7 @@ struct Params {
   unsigned long long* start_ns;
   int* flags;  // [0] budget expired, [1] inversion failure, [2] queue overflows
   unsigned long long* hits;  // sample-0 matches sent to verification (may be null)
+  unsigned long long* preq;  // per-CTA queues of sample-0 matches, [grid][kPreG][2] (may be null)
   unsigned long long total_units;
   unsigned long long unit_offset;  // this shard's first unit (multi-GPU)
   unsigned long long unit_stride;  // number of shards (0 is read as 1)
@@ -201,6 +213,8 @@ struct alignas(16) Smem {
   int inst_idx;
   int pad_[3];
   unsigned long long queue[kQueue];
+  unsigned long long pre_c[kPre], pre_v[kPre];  // sample-0 matches: context, bottom index
+  int pn;
   unsigned long long unit;
   unsigned long long unit_local;  // unit index within its spine
   int qn;
@@ -209,6 +223,9 @@ struct alignas(16) Smem {
   int skip;
   int task_idx;
   int next_task;
+  // thread 0's last lookups: the unit ranges of the last task and spine
+  unsigned long long lk_task_lo, lk_task_hi, lk_item_lo, lk_item_hi;
+  int lk_task, lk_item;
   char post[kThreads / 32][kMaxSize + 8];
 };
 
@@ -419,15 +436,25 @@ __device__ void verify_queue(const InstDesc<W>& d, Smem& sm, const W* s_in, cons
 // and return its rank base; optionally fetch the small values.
 template <class W>
 __device__ __forceinline__ unsigned long long decode_context(const InstDesc<W>& d, const Item& it,
-                                                             unsigned long long c, W* wl) {
+                                                             unsigned long long c, W* wl,
+                                                             const W* const* tabs = nullptr) {
+  if (!tabs) tabs = d.tab;
   unsigned long long rank = it.base;
   for (int l = it.depth - 1; l >= 0; --l) {
     const Level& L = it.lv[l];
     if (L.kind != 0) continue;
-    const unsigned long long idx = c % L.nsmall;
-    c /= L.nsmall;
+    unsigned long long idx;
+    if ((c >> 32) == 0 && (L.nsmall >> 32) == 0) {  // 32-bit division when it fits
+      const unsigned c32 = (unsigned)c, n32 = (unsigned)L.nsmall;
+      const unsigned q = c32 / n32;
+      idx = c32 - q * n32;
+      c = q;
+    } else {
+      idx = c % L.nsmall;
+      c /= L.nsmall;
+    }
     rank += idx * L.coef;
-    if (wl) wl[l] = d.tab[L.ts][idx];
+    if (wl) wl[l] = tabs[L.ts][idx];
   }
   return rank;
 }
@@ -462,6 +489,93 @@ __device__ __forceinline__ W eval_explicit(const Explicit<W>& X, const W* w, W x
 // One work unit: kR contexts per thread x a strided share of the bottom
 // values.  Loads are 16-byte vectors of the bottom table, four in flight per
 // thread.  FUSED units take their contexts from the materialised list.
+// Further filters for a sample-0 match (context c, bottom index v): the same
+// spine inverted against samples 1..kExtra, from their value tables.  Exact
+// like the first (a rejected candidate does not match that sample); they
+// spare the unrank-and-evaluate verification the candidates whose sample-0
+// mask is sparse (spines under nested & and |).  Passes what it cannot decide.
+template <class W>
+__device__ __forceinline__ bool extra_check(const InstDesc<W>& d, const Item& it, unsigned long long c,
+                                            unsigned long long v) {
+  for (int j = 0; j < kExtra; ++j) {
+    const W* const* tb = d.tabx[j];
+    if (!tb[it.bottom]) break;
+    for (int l = 0; l < it.depth; ++l)  // filter tables may stop below the tabled size
+      if (it.lv[l].kind == 0 && !tb[it.lv[l].ts]) return true;
+    W wl[kMaxDepth];
+    decode_context<W>(d, it, c, wl, tb);
+    W m = (W)~W(0), k = d.targetx[j];
+    bool ok = true;
+    for (int l = 0; l < it.inv && ok; ++l) ok = invert_level<W>(it.lv[l], wl[l], m, k);
+    if (!ok) return true;
+    W y = tb[it.bottom][v];
+    for (int l = it.depth - 1; l >= it.inv; --l) {  // explicit levels, bottom-up
+      const Level& Lv = it.lv[l];
+      y = level_apply<W>(Lv.kind, Lv.op, Lv.small_left, Lv.eps, (W)Lv.c, wl[l], y);
+    }
+    if ((W)(y & m) != k) return false;
+  }
+  return true;
+}
+
+// Rank of candidate (context c, bottom index v) of the item; for a fused
+// item c indexes the materialised contexts.
+template <class W>
+__device__ __forceinline__ unsigned long long candidate_rank(const Params<W>& p, const InstDesc<W>& d,
+                                                             const Item& it, unsigned long long c,
+                                                             unsigned long long v) {
+  if (it.fused) {
+    const Ctx<W> cx = p.ctxs[it.ctx_off + c];
+    return cx.base + v * p.sitems[cx.member].coefv;
+  }
+  return decode_context<W>(d, it, c, nullptr) + v * it.coefv;
+}
+
+// A sample-0 match is queued (context, bottom index) for the filter samples,
+// which run after the work unit (filter_queue), so that the search loop keeps
+// only this small inlined step; on overflow it goes straight to verification.
+template <class W>
+__device__ __forceinline__ void pre_push(const Params<W>& p, const InstDesc<W>& d, Smem& sm, const Item& it,
+                                         unsigned long long c, unsigned long long v, const W* s_in,
+                                         const W* s_out) {
+  const int i = atomicAdd(&sm.pn, 1);
+  if (p.preq) {
+    if (i < kPreG) {
+      unsigned long long* e = p.preq + ((size_t)blockIdx.x * kPreG + i) * 2;
+      e[0] = c;
+      e[1] = v;
+      return;
+    }
+  } else if (i < kPre) {
+    sm.pre_c[i] = c;
+    sm.pre_v[i] = v;
+    return;
+  }
+  push_hit<W>(p, d, sm, s_in, s_out, candidate_rank<W>(p, d, it, c, v));
+}
+
+// All threads: run the filter samples on the queued sample-0 matches of the
+// unit's item and queue the survivors for verification.
+template <class W>
+__device__ void filter_queue(const Params<W>& p, const InstDesc<W>& d, Smem& sm, const W* s_in,
+                             const W* s_out) {
+  const int n = min(sm.pn, p.preq ? kPreG : kPre);
+  const Item& it = sm.item;
+  const unsigned long long* gq = p.preq ? p.preq + (size_t)blockIdx.x * kPreG * 2 : nullptr;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const unsigned long long c = gq ? gq[2 * i] : sm.pre_c[i];
+    const unsigned long long v = gq ? gq[2 * i + 1] : sm.pre_v[i];
+    bool pass;
+    if (it.fused) {
+      const Ctx<W> cx = p.ctxs[it.ctx_off + c];
+      pass = extra_check<W>(d, p.sitems[cx.member], cx.c, v);
+    } else {
+      pass = extra_check<W>(d, it, c, v);
+    }
+    if (pass) push_hit<W>(p, d, sm, s_in, s_out, candidate_rank<W>(p, d, it, c, v));
+  }
+}
+
 template <class W, int E, bool FULL, bool FUSED>
 __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm, const Item& it,
                              unsigned long long local, const W* s_in, const W* s_out) {
@@ -538,48 +652,16 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
         W y = xs[e];
         if (E > 0) y = eval_explicit<W, E>(X, WX[r], y);
         const bool h = FULL ? (y == K[r]) : ((W)(y & M[r]) == K[r]);
-        if (!h) continue;
-        unsigned long long rank;
-        if (FUSED) {
-          const Ctx<W> cx = p.ctxs[it.ctx_off + c0 + r];
-          rank = cx.base + v * cx.coefv;
-        } else {
-          rank = decode_context<W>(d, it, c0 + r, nullptr) + v * it.coefv;
-        }
-        push_hit<W>(p, d, sm, s_in, s_out, rank);
+        if (h) pre_push<W>(p, d, sm, it, c0 + r, v, s_in, s_out);
       }
     }
   };
 
+  // The bottom values are streamed with four 16-byte loads in flight (one
+  // with explicit levels, for code size).
   unsigned long long q = q0 + lane;
   const unsigned long long step = (unsigned long long)L;
-  if (E == 0) {  // four loads in flight; explicit levels keep one (code size)
-#if SIMBA_PIPE
-    // software pipeline: the next four loads are issued before the current
-    // four values are tested
-    const unsigned long long span = 4 * step;
-    if (q + 3 * step < q1) {
-      uint4 a0 = __ldg(V4 + q), a1 = __ldg(V4 + q + step), a2 = __ldg(V4 + q + 2 * step),
-            a3 = __ldg(V4 + q + 3 * step);
-      q += span;
-      for (; q + 3 * step < q1; q += span) {
-        const uint4 b0 = __ldg(V4 + q), b1 = __ldg(V4 + q + step), b2 = __ldg(V4 + q + 2 * step),
-                    b3 = __ldg(V4 + q + 3 * step);
-        test(a0, q - span);
-        test(a1, q - span + step);
-        test(a2, q - span + 2 * step);
-        test(a3, q - span + 3 * step);
-        a0 = b0;
-        a1 = b1;
-        a2 = b2;
-        a3 = b3;
-      }
-      test(a0, q - span);
-      test(a1, q - span + step);
-      test(a2, q - span + 2 * step);
-      test(a3, q - span + 3 * step);
-    }
-#else
+  if (E == 0) {
     for (; q + 3 * step < q1; q += 4 * step) {
       const uint4 a0 = __ldg(V4 + q);
       const uint4 a1 = __ldg(V4 + q + step);
@@ -590,7 +672,6 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
       test(a2, q + 2 * step);
       test(a3, q + 3 * step);
     }
-#endif
   }
   for (; q < q1; q += step) test(__ldg(V4 + q), q);
 }
@@ -629,7 +710,8 @@ __global__ void __launch_bounds__(256) materialize_kernel(Params<W> p, Ctx<W>* o
     W wl[kMaxDepth];
     Ctx<W> cx;
     cx.base = decode_context<W>(d, it, c, wl);
-    cx.coefv = it.coefv;
+    cx.member = (unsigned)lo;
+    cx.c = (unsigned)c;
     W m = (W)~W(0), k = d.target;
     for (int l = 0; l < it.depth; ++l)
       if (!invert_level<W>(it.lv[l], wl[l], m, k)) atomicOr(&p.flags[1], 1);
@@ -663,7 +745,9 @@ __device__ void process_unit_generic(const Params<W>& p, const InstDesc<W>& d, S
         const Level& Lv = it.lv[l];
         y = level_apply<W>(Lv.kind, Lv.op, Lv.small_left, Lv.eps, (W)Lv.c, wl[l], y);
       }
-      if (y == d.target) push_hit<W>(p, d, sm, s_in, s_out, rb + v * it.coefv);
+      if (y != d.target) continue;
+      (void)rb;
+      pre_push<W>(p, d, sm, it, c, v, s_in, s_out);
     }
   }
 }
@@ -732,9 +816,12 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
   const InstDesc<W>& d = *reinterpret_cast<const InstDesc<W>*>(sm.desc);
   if (threadIdx.x == 0) {
     sm.qn = 0;
+    sm.pn = 0;
     sm.item_idx = -1;
     sm.task_idx = -2;
     sm.inst_idx = -1;
+    sm.lk_task = -1;
+    sm.lk_item = -1;
   }
   __syncthreads();
   for (;;) {
@@ -753,10 +840,18 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
         int ilo = 0, ihi = p.nitems - 1, inst = -1, task = -1;
         if (p.tasks) {  // batch: task, then the spine inside its shared list
           int lo = 0, hi = p.ntasks - 1;
-          while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (p.tasks[mid].unit_begin <= u) lo = mid;
-            else hi = mid - 1;
+          if (sm.lk_task >= 0 && u >= sm.lk_task_lo && u < sm.lk_task_hi) {
+            lo = sm.lk_task;  // units of one task are consecutive: usually a hit
+          } else {
+            while (lo < hi) {
+              const int mid = (lo + hi + 1) >> 1;
+              if (p.tasks[mid].unit_begin <= u) lo = mid;
+              else hi = mid - 1;
+            }
+            sm.lk_task = lo;
+            sm.lk_task_lo = p.tasks[lo].unit_begin;
+            sm.lk_task_hi = lo + 1 < p.ntasks ? p.tasks[lo + 1].unit_begin : p.total_units;
+            sm.lk_item = -1;
           }
           task = lo;
           const Task tk = p.tasks[lo];
@@ -773,10 +868,17 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
             ihi = (int)(td.item_off + tb.item[b + 1]) - 1;
           }
         }
-        while (ilo < ihi) {
-          const int mid = (ilo + ihi + 1) >> 1;
-          if (p.items[mid].unit_begin <= local) ilo = mid;
-          else ihi = mid - 1;
+        if (sm.lk_item >= ilo && sm.lk_item <= ihi && local >= sm.lk_item_lo && local < sm.lk_item_hi) {
+          ilo = sm.lk_item;
+        } else {
+          while (ilo < ihi) {
+            const int mid = (ilo + ihi + 1) >> 1;
+            if (p.items[mid].unit_begin <= local) ilo = mid;
+            else ihi = mid - 1;
+          }
+          sm.lk_item = ilo;
+          sm.lk_item_lo = p.items[ilo].unit_begin;
+          sm.lk_item_hi = sm.lk_item_lo + item_units(p.items[ilo]);
         }
         sm.next_item = ilo;
         sm.next_task = task;
@@ -817,14 +919,33 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
         if (threadIdx.x == 0) sm.inst_idx = (int)it.inst;
       }
       const unsigned long long local = sm.unit_local;
-      dispatch_unit<W>(p, d, sm, it, local, s_in, s_out);
-      if (threadIdx.x == 0) {
-        const unsigned long long cblk = local / it.vblocks, vblk = local % it.vblocks;
-        const unsigned long long c0 = cblk * it.cb, c1 = umin64(c0 + it.cb, it.nctx);
-        const unsigned long long v0 = vblk * it.vb, v1 = umin64(v0 + it.vb, it.nv);
-        atomicAdd(p.evaluated, (c1 - c0) * (v1 - v0));
+      const unsigned long long cu = local / it.vblocks, vblk = local - cu * it.vblocks;
+      const unsigned long long cpu = it.cpu ? it.cpu : 1;
+      const unsigned long long b0 = cu * cpu, b1 = umin64(b0 + cpu, it.cblocks);
+      for (unsigned long long b = b0; b < b1; ++b) {
+        dispatch_unit<W>(p, d, sm, it, b * it.vblocks + vblk, s_in, s_out);
+        if (threadIdx.x == 0) {
+          const unsigned long long c0 = b * it.cb, c1 = umin64(c0 + it.cb, it.nctx);
+          const unsigned long long v0 = vblk * it.vb, v1 = umin64(v0 + it.vb, it.nv);
+          atomicAdd(p.evaluated, (c1 - c0) * (v1 - v0));
+        }
+        if (b + 1 < b1) {  // filter and verify this block's matches before the next one
+          __syncthreads();
+          if (sm.pn > 0) filter_queue<W>(p, d, sm, s_in, s_out);
+          __syncthreads();
+          if (sm.qn > 0) verify_queue<W>(d, sm, s_in, s_out);
+          __syncthreads();
+          if (threadIdx.x == 0) {
+            if (p.hits && sm.qn) atomicAdd(p.hits, (unsigned long long)sm.qn);
+            sm.qn = 0;
+            sm.pn = 0;
+          }
+          __syncthreads();
+        }
       }
     }
+    __syncthreads();
+    if (sm.pn > 0) filter_queue<W>(p, d, sm, s_in, s_out);
     __syncthreads();
     if (sm.qn > 0) verify_queue<W>(d, sm, s_in, s_out);
     __syncthreads();
@@ -832,6 +953,7 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
       if (!sm.skip && d.ns) atomicMax(d.ns + 1, globaltimer_ns());
       if (p.hits && sm.qn) atomicAdd(p.hits, (unsigned long long)sm.qn);
       sm.qn = 0;
+      sm.pn = 0;
       sm.item_idx = ni;
       sm.task_idx = nt;
     }
@@ -925,6 +1047,22 @@ __global__ void build_batch_kernel(const BuildJob<W>* jobs, int njobs, unsigned 
 }
 
 static __global__ void stamp_start_kernel(unsigned long long* t) { *t = globaltimer_ns(); }
+
+// Batch start: instance i's terminals on sample j (row ns*i + j of src, maxK
+// wide) go to its V_1 table at byte offset dst[ns*i + j] (~0: no such table).
+template <class W>
+__global__ void scatter_terminals_kernel(const W* src, const unsigned long long* dst, const int* k,
+                                         char* base, int n, int maxK, int ns) {
+  const unsigned long long total = (unsigned long long)ns * n * maxK;
+  for (unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long row = g / maxK;
+    const int q = (int)(g - row * maxK);
+    const int i = (int)(row / ns);
+    if (q >= k[i] || dst[row] == ~0ULL) continue;
+    reinterpret_cast<W*>(base + dst[row])[q] = src[g];
+  }
+}
 
 // ------------------------------------------------------------------ host side
 
@@ -1106,6 +1244,15 @@ static inline void finish_layout(Item& it, int threads, uint64_t unit_target = 1
   if (vb > nv_al) vb = nv_al;
   it.vb = vb;
   it.vblocks = (it.nv + vb - 1) / vb;
+  // small bottoms: one context block holds few candidates, so a unit takes
+  // several blocks and the per-unit queue and lookup cost is amortised
+  it.cpu = 1;
+  if (it.vblocks == 1) {
+    const uint64_t per = (uint64_t)it.cb * std::max<uint64_t>(it.nv, 1);
+    if (per < unit_target)
+      it.cpu = (uint16_t)std::min<uint64_t>({unit_target / per, it.cblocks, 65535ULL});
+    if (it.cpu == 0) it.cpu = 1;
+  }
 }
 
 static inline void finish_item(Item& it, int threads, uint64_t mask) {
@@ -1243,11 +1390,14 @@ class Search final : public SearchSession {
     SB_CUDA(d_insts_.reserve(sizeof(InstDesc<W>)));
 
     // table budget -> largest tabled size
-    const int64_t budget = o_.table_bytes > 0 ? o_.table_bytes : (4LL << 30);
+    const int64_t budget = o_.table_bytes > 0 ? o_.table_bytes : (8LL << 30);
     uint64_t total = 0;
     Tcap_ = 0;
+    // every tabled size has the tables of all samples (sample 0 and the
+    // filter samples): a spine touching a size without filter tables would
+    // send its sparse-mask matches to verification unfiltered
     for (int t = 1; t <= count_ok_max_ && t <= 20; ++t) {
-      const uint64_t bytes = padded(ct_.n[t][8]) * sizeof(W);
+      const uint64_t bytes = padded(ct_.n[t][8]) * sizeof(W) * nsamp();
       if (total + bytes > (uint64_t)budget) break;
       total += bytes;
       Tcap_ = t;
@@ -1263,6 +1413,7 @@ class Search final : public SearchSession {
     int occ = 1;
     SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, spine_kernel<W>, kThreads, smem_bytes_));
     grid_ = sms_ * std::max(occ, 1);
+    SB_CUDA(d_preq_.reserve((size_t)grid_ * kPreG * 16));
     int occn = 1;
     SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occn, naive_kernel<W>, kThreads, smem_bytes_));
     grid_naive_ = sms_ * std::max(occn, 1);
@@ -1301,25 +1452,30 @@ class Search final : public SearchSession {
  private:
   static uint64_t padded(uint64_t n) { return (n + 63) / 64 * 64 + 64; }
 
-  W* tab(int t) const { return d_tabs_[t].as<W>(); }
+  // V_t on sample j (j = 0, and the filter samples 1..kExtra that exist): one
+  // allocation per size t holds the tables of all samples
+  W* tab(int t, int j = 0) const { return d_tabs_[t].as<W>() + (size_t)j * padded(ct_.n[t][8]); }
+  int nsamp() const { return std::min(h_.S, kExtra + 1); }
 
   // Build V_{built+1} .. V_t (each entry one operator over smaller tables).
   int ensure_tables(int t) {
     for (int s = built_ + 1; s <= t; ++s) {
-      SB_CUDA(d_tabs_[s].reserve(padded(ct_.n[s][8]) * sizeof(W)));
-      W* o = tab(s);
-      if (s == 1) {
-        std::vector<W> v(padded(h_.k), 0);
-        for (int j = 0; j < h_.k; ++j) v[j] = (W)h_.in[j];
-        SB_CUDA(cudaMemcpyAsync(o, v.data(), v.size() * sizeof(W), cudaMemcpyHostToDevice, stream_));
-      } else {
+      SB_CUDA(d_tabs_[s].reserve(padded(ct_.n[s][8]) * sizeof(W) * nsamp()));
+      for (int j = 0; j < nsamp(); ++j) {
+        W* o = tab(s, j);
+        if (s == 1) {
+          std::vector<W> v(padded(h_.k), 0);
+          for (int q = 0; q < h_.k; ++q) v[q] = (W)h_.in[(size_t)j * h_.k + q];
+          SB_CUDA(cudaMemcpyAsync(o, v.data(), v.size() * sizeof(W), cudaMemcpyHostToDevice, stream_));
+          continue;
+        }
         uint64_t off = 0;
         const int sub = s - 1;
         for (int op = 0; op < 8; ++op) {
           if (is_unary(op)) {
             const uint64_t n = ct_.n[sub][8];
             const int blocks = (int)std::min<uint64_t>((n + 255) / 256, (uint64_t)sms_ * 16);
-            build_unary_kernel<W><<<blocks, 256, 0, stream_>>>(o + off, tab(sub), n, op);
+            build_unary_kernel<W><<<blocks, 256, 0, stream_>>>(o + off, tab(sub, j), n, op);
             ++launches_;
             off += n;
             continue;
@@ -1329,7 +1485,8 @@ class Search final : public SearchSession {
             const uint64_t na = ct_.n[f][8], nb = ct_.n[sub - f][8];
             const uint64_t n = na * nb;
             const int blocks = (int)std::min<uint64_t>((n + 255) / 256, (uint64_t)sms_ * 16);
-            build_binary_kernel<W><<<blocks, 256, 0, stream_>>>(o + off, tab(f), tab(sub - f), na, nb, op);
+            build_binary_kernel<W><<<blocks, 256, 0, stream_>>>(o + off, tab(f, j), tab(sub - f, j),
+                                                               na, nb, op);
             ++launches_;
             off += n;
           }
@@ -1345,7 +1502,11 @@ class Search final : public SearchSession {
   Params<W> params(int s) {
     InstDesc<W> d;
     memset(&d, 0, sizeof(d));
-    for (int t = 1; t <= built_; ++t) d.tab[t] = tab(t);
+    for (int t = 1; t <= built_; ++t) {
+      d.tab[t] = tab(t);
+      for (int j = 1; j < nsamp(); ++j) d.tabx[j - 1][t] = tab(t, j);
+    }
+    for (int j = 1; j < nsamp(); ++j) d.targetx[j - 1] = (W)h_.out[j];
     d.in = d_in_.as<W>();
     d.out = d_out_.as<W>();
     d.counts = d_counts_.as<unsigned long long>();
@@ -1368,6 +1529,7 @@ class Search final : public SearchSession {
     p.start_ns = sc + 3;
     p.flags = reinterpret_cast<int*>(sc + 4);
     p.hits = sc + 6;
+    p.preq = d_preq_.as<unsigned long long>();
     p.maxS = h_.S;
     p.maxK = h_.k;
     p.budget_ns = o_.budget_s > 0 ? (unsigned long long)(o_.budget_s * 1e9) : 0;
@@ -1450,7 +1612,7 @@ class Search final : public SearchSession {
       uint64_t units = 0;
       for (auto& it : items) {
         it.unit_begin = units;
-        units += it.cblocks * it.vblocks;
+        units += item_units(it);
       }
       SB_CUDA(d_items_.reserve(items.size() * sizeof(Item)));
       SB_CUDA(cudaMemcpyAsync(d_items_.p, items.data(), items.size() * sizeof(Item),
@@ -1617,8 +1779,8 @@ class Search final : public SearchSession {
   uint64_t alg_ops_ = 0;
   int sms_ = 0, grid_ = 0, grid_naive_ = 0;
   size_t smem_bytes_ = 0;
-  DevBuf d_in_, d_out_, d_counts_, d_scal_, d_items_, d_small_, d_ctx_, d_insts_;
-  DevBuf d_tabs_[kMaxSize + 1];  // V_t, allocated when size t is first built
+  DevBuf d_in_, d_out_, d_counts_, d_scal_, d_items_, d_small_, d_ctx_, d_insts_, d_preq_;
+  DevBuf d_tabs_[kMaxSize + 1];  // V_t of every sample, allocated when size t is first built
   unsigned long long h_scal_[8] = {};
   int Tcap_ = 0, built_ = 0, last_T_ = 0;
 };
@@ -1712,19 +1874,24 @@ class Batch {
     std::vector<std::array<uint64_t, kMaxSize + 1>> toff(n);
     uint64_t tab_total = 0, smp_total = 0;
     auto padded = [](uint64_t x) { return (x + 63) / 64 * 64 + 64; };
+    std::vector<uint64_t> tab_sz(n);
+    std::vector<int> nsamp(n);
     for (int i = 0; i < n; ++i) {
       const CountTable& ct = cts_[ct_of[i]];
-      uint64_t tot = 0;
+      nsamp[i] = std::min(hs_[i].S, kExtra + 1);  // sample-0 tables and the filter samples'
+      const uint64_t ns = (uint64_t)nsamp[i];
+      uint64_t tot = 0;  // every tabled size has the tables of all samples
       T[i] = 0;
       for (int t = 1; t <= ct.max_size && t <= 16; ++t) {
         const uint64_t b = padded(ct.n[t][8]) * sizeof(W);
-        if (t > 1 && tot + b > (uint64_t)inst_budget_) break;
+        if (t > 1 && (tot + b) * ns > (uint64_t)inst_budget_) break;
         toff[i][t] = tot;
         tot += b;
         T[i] = t;
       }
       tab_off[i] = tab_total;
-      tab_total += tot;
+      tab_sz[i] = tot;
+      tab_total += tot * ns;
       in_off[i] = smp_total;
       smp_total += ((uint64_t)hs_[i].S * hs_[i].k * sizeof(W) + 15) / 16 * 16;
       out_off[i] = smp_total;
@@ -1749,26 +1916,45 @@ class Batch {
       for (size_t j = 0; j < cts_.size(); ++j)
         memcpy(cta.data() + j * (kMaxSize + 1) * kCols, cts_[j].n, sizeof(cts_[j].n));
       SB_CUDA(cudaMemcpy(d_cts_.p, cta.data(), cta.size() * 8, cudaMemcpyHostToDevice));
-      // V_1 of every instance: the terminals on sample 0
-      std::vector<W> v1;
+      // V_1 of every instance: the terminals on samples 0 and 1, gathered
+      // into one upload and scattered to the instances' tables on the device
+      constexpr int NS = kExtra + 1;
+      std::vector<W> v1((size_t)NS * n * maxK, 0);
+      std::vector<unsigned long long> dst((size_t)NS * n, ~0ULL);
+      std::vector<int> kk(n);
       for (int i = 0; i < n; ++i) {
-        v1.assign(padded(hs_[i].k), 0);
-        for (int j = 0; j < hs_[i].k; ++j) v1[j] = (W)hs_[i].in[j];
-        SB_CUDA(cudaMemcpyAsync(d_tab_.as<char>() + tab_off[i] + toff[i][1], v1.data(),
-                                v1.size() * sizeof(W), cudaMemcpyHostToDevice, stream_));
-        SB_CUDA(cudaStreamSynchronize(stream_));
+        kk[i] = hs_[i].k;
+        for (int j = 0; j < nsamp[i]; ++j) {
+          dst[(size_t)NS * i + j] = tab_off[i] + (uint64_t)j * tab_sz[i] + toff[i][1];
+          for (int q = 0; q < hs_[i].k; ++q)
+            v1[((size_t)NS * i + j) * maxK + q] = (W)hs_[i].in[(size_t)j * hs_[i].k + q];
+        }
       }
+      DevBuf d_v1, d_dst, d_kk;
+      SB_CUDA(d_v1.reserve(v1.size() * sizeof(W)));
+      SB_CUDA(d_dst.reserve(dst.size() * 8));
+      SB_CUDA(d_kk.reserve(kk.size() * sizeof(int) + 16));
+      SB_CUDA(cudaMemcpy(d_v1.p, v1.data(), v1.size() * sizeof(W), cudaMemcpyHostToDevice));
+      SB_CUDA(cudaMemcpy(d_dst.p, dst.data(), dst.size() * 8, cudaMemcpyHostToDevice));
+      SB_CUDA(cudaMemcpy(d_kk.p, kk.data(), kk.size() * sizeof(int), cudaMemcpyHostToDevice));
+      const unsigned long long nw = (unsigned long long)NS * n * maxK;
+      scatter_terminals_kernel<W><<<(int)std::min<unsigned long long>((nw + 255) / 256, 65535), 256, 0,
+                                    stream_>>>(d_v1.as<W>(), d_dst.as<unsigned long long>(),
+                                               d_kk.as<int>(), d_tab_.as<char>(), n, maxK, NS);
+      SB_CUDA(cudaGetLastError());
+      SB_CUDA(cudaStreamSynchronize(stream_));
     }
     std::vector<int> size(n), built(n, 1);
     const int first = o_.size_range ? 1 : 2;
     const int last = o_.size_range ? max_size : max_size - 1;
     for (int i = 0; i < n; ++i) size[i] = first;
-    std::vector<char> active(n, 1), inround(n, 0);
+    std::vector<char> active(n, 1), inround(n, 0), ran(n, 0);
     std::vector<double> swept(n, 0.0);  // candidates of the sizes already searched
     if (first > last)
       for (int i = 0; i < n; ++i) active[i] = 0, (*outs)[i].status = SIMBA_NOT_FOUND;
-    auto tabp = [&](int i, int t) {
-      return reinterpret_cast<const W*>(d_tab_.as<char>() + tab_off[i] + toff[i][t]);
+    auto tabp = [&](int i, int t, int j = 0) {  // sample j's V_t of instance i
+      return reinterpret_cast<const W*>(d_tab_.as<char>() + tab_off[i] + (uint64_t)j * tab_sz[i] +
+                                        toff[i][t]);
     };
     auto next_cost = [&](int i) { return swept[i] + (double)cts_[ct_of[i]].n[size[i]][8]; };
     const size_t smem = ((sizeof(Smem) + 15) & ~size_t(15)) +
@@ -1778,6 +1964,7 @@ class Batch {
     int occ = 1;
     SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, spine_kernel<W>, kThreads, smem));
     const int grid = sms * std::max(occ, 1);
+    SB_CUDA(d_preq_.reserve((size_t)grid * kPreG * 16));
     SB_CUDA(d_ns_.reserve((size_t)n * 16 + 16));
     SB_CUDA(cudaMemsetAsync(d_ns_.p, 0, (size_t)n * 16, stream_));
     std::vector<unsigned long long> ns(2 * (size_t)n + 2);
@@ -1830,20 +2017,22 @@ class Batch {
         const int want = std::min(size[i], T[i]);
         const CountTable& ct = cts_[ct_of[i]];
         for (int t = built[i] + 1; t <= want; ++t) {
-          uint64_t off = 0;
           const int sub = t - 1;
-          W* o = const_cast<W*>(tabp(i, t));
-          for (int op = 0; op < 8; ++op) {
-            if (is_unary(op)) {
-              build_jobs_.push_back({o + off, tabp(i, sub), nullptr, ct.n[sub][8], 1, op, 0});
-              off += ct.n[sub][8];
-              continue;
-            }
-            const int fmax = is_commutative(op) ? sub / 2 : sub - 1;
-            for (int f = 1; f <= fmax; ++f) {
-              const uint64_t na = ct.n[f][8], nb = ct.n[sub - f][8];
-              build_jobs_.push_back({o + off, tabp(i, f), tabp(i, sub - f), na, nb, op, 0});
-              off += na * nb;
+          for (int j = 0; j < nsamp[i]; ++j) {
+            uint64_t off = 0;
+            W* o = const_cast<W*>(tabp(i, t, j));
+            for (int op = 0; op < 8; ++op) {
+              if (is_unary(op)) {
+                build_jobs_.push_back({o + off, tabp(i, sub, j), nullptr, ct.n[sub][8], 1, op, 0});
+                off += ct.n[sub][8];
+                continue;
+              }
+              const int fmax = is_commutative(op) ? sub / 2 : sub - 1;
+              for (int f = 1; f <= fmax; ++f) {
+                const uint64_t na = ct.n[f][8], nb = ct.n[sub - f][8];
+                build_jobs_.push_back({o + off, tabp(i, f, j), tabp(i, sub - f, j), na, nb, op, 0});
+                off += na * nb;
+              }
             }
           }
           built[i] = t;
@@ -1864,10 +2053,11 @@ class Batch {
         ++*launches;
         SB_CUDA(cudaGetLastError());
       }
-      // 2. tasks on the shared spine lists.  Plain: one per instance, the
-      // cheapest first.  Guided: one per (instance, shape-class bucket),
-      // ordered by prior probability per unit of work across all instances
-      // of the round, so the likeliest spines of every instance run first.
+      // 2. tasks on the shared spine lists, instances cheapest first.  Plain:
+      // one task per instance.  Guided: one per (instance, shape-class
+      // bucket), an instance's buckets by prior probability per unit of
+      // work, so each instance reaches its likeliest spines first and no
+      // instance waits for another's guesses.
       tasks_.clear();
       mtasks_.clear();
       const float* priors = o_.class_prior;  // n x 64 in batch mode
@@ -1881,15 +2071,25 @@ class Batch {
         uint64_t ctx_base, units;
       };
       std::vector<Pending> pend;
+      // materialised contexts must fit in free memory: the most expensive
+      // instances of the round wait for a later round if they do not
+      size_t mem_free = 0, mem_total = 0;
+      SB_CUDA(cudaMemGetInfo(&mem_free, &mem_total));
+      const uint64_t room = mem_free + d_ctx_.bytes;
+      const uint64_t ctx_room = room > (1ULL << 30) ? (room - (1ULL << 30)) / sizeof(Ctx<W>) : 0;
       for (int i : order) {
+        ran[i] = 0;
         const CountTable& ct = cts_[ct_of[i]];
         const int ul = hs_[i].unit_log2 > 0 ? std::min(hs_[i].unit_log2, 40) : 0;
         const ItemTemplate& tp = get_template(ct, std::min(T[i], size[i]), size[i], mask,
                                               ul ? 1ULL << ul : unit_target_, guided);
         if (!tp.ok || tp.units == 0) {
           naive_insts.push_back(i);
+          ran[i] = 1;
           continue;
         }
+        if (ctx_base + tp.nctxs > ctx_room && !pend.empty()) continue;  // deferred
+        ran[i] = 1;
         Task mt;
         memset(&mt, 0, sizeof(mt));
         mt.ctx_base = ctx_base;
@@ -1897,8 +2097,9 @@ class Batch {
         mt.tmpl = (unsigned)tp.id;
         mt.bucket = -1;
         if (tp.nctxs) mtasks_.push_back(mt);
-        if (guided) {
+        if (guided) {  // this instance's buckets, likeliest per unit of work first
           const float* pr = priors + (size_t)i * 64;
+          const size_t first = pend.size();
           for (int b = 0; b < 64; ++b) {
             if (tp.bucket_units[b] == 0) continue;
             // a unary-chain bucket holds both ~- and neg-rooted chains
@@ -1906,15 +2107,14 @@ class Batch {
             pend.push_back({-(std::max(pb, 1e-12) / (double)tp.bucket_units[b]), i, b,
                             (unsigned)tp.id, ctx_base, tp.bucket_units[b]});
           }
+          std::stable_sort(pend.begin() + first, pend.end(),
+                           [](const Pending& a, const Pending& b) { return a.key < b.key; });
         } else {
           pend.push_back({0.0, i, -1, (unsigned)tp.id, ctx_base, tp.units});
         }
         ctx_base += tp.nctxs;
         *alg_ops += tp.alg;
       }
-      if (guided)
-        std::stable_sort(pend.begin(), pend.end(),
-                         [](const Pending& a, const Pending& b) { return a.key < b.key; });
       for (const Pending& q : pend) {
         Task tk;
         memset(&tk, 0, sizeof(tk));
@@ -1946,7 +2146,11 @@ class Batch {
       for (int i = 0; i < n; ++i) {
         InstDesc<W>& d = desc[i];
         memset(&d, 0, sizeof(d));
-        for (int t = 1; t <= built[i]; ++t) d.tab[t] = tabp(i, t);
+        for (int t = 1; t <= built[i]; ++t) {
+          d.tab[t] = tabp(i, t);
+          for (int j = 1; j < nsamp[i]; ++j) d.tabx[j - 1][t] = tabp(i, t, j);
+        }
+        for (int j = 1; j < nsamp[i]; ++j) d.targetx[j - 1] = (W)hs_[i].out[j];
         d.in = reinterpret_cast<const W*>(d_smp_.as<char>() + in_off[i]);
         d.out = reinterpret_cast<const W*>(d_smp_.as<char>() + out_off[i]);
         d.counts = d_cts_.as<unsigned long long>() + (size_t)ct_of[i] * (kMaxSize + 1) * kCols;
@@ -1971,6 +2175,7 @@ class Batch {
       p.start_ns = sc + 3;
       p.flags = reinterpret_cast<int*>(sc + 4);
       p.hits = sc + 6;
+      p.preq = d_preq_.as<unsigned long long>();
       p.maxS = maxS;
       p.maxK = maxK;
       p.stop_on_match = guided ? 2 : 1;  // guided: any verified match of the size
@@ -2040,6 +2245,7 @@ class Batch {
       const double now = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
       // 4. retire solved instances, advance the others
       for (int i : order) {
+        if (!ran[i]) continue;
         Out& r = (*outs)[i];
         const CountTable& ct = cts_[ct_of[i]];
         const int s = size[i];
@@ -2079,8 +2285,10 @@ class Batch {
         }
       }
       if (o_.verbose) {
-        int solved = 0, smin = kMaxSize, smax = 0;
+        int solved = 0, smin = kMaxSize, smax = 0, nran = 0;
         for (int i : order) {
+          if (!ran[i]) continue;
+          ++nran;
           solved += best[i] != ~0ULL;
           smin = std::min(smin, size[i] - (best[i] == ~0ULL ? 1 : 0));
           smax = std::max(smax, size[i] - (best[i] == ~0ULL ? 1 : 0));
@@ -2089,7 +2297,7 @@ class Batch {
                 "round %3d | t %8.3f s | insts %6zu (sizes %d-%d) | tasks %7zu | units %10llu | "
                 "ctxs %10llu | naive %4zu | evaluated %.3e | hits %.3e | kernels %9.3f ms | "
                 "solved %5d%s\n",
-                *rounds, now, order.size(), smin, smax, tasks_.size(), (unsigned long long)units,
+                *rounds, now, (size_t)nran, smin, smax, tasks_.size(), (unsigned long long)units,
                 (unsigned long long)ctx_base, naive_insts.size(), (double)hs[2], (double)hs[6], kms,
                 solved, fl[0] ? " | budget" : "");
       }
@@ -2161,15 +2369,25 @@ class Batch {
         for (auto& it : items) it.prio = (float)bucket_of(it, s);
       fuse_small(items, &tp.small, &tp.nctxs, ct, 1ULL << 22, guided);
       for (auto& it : items) finish_layout(it, kThreads, unit_target);
+      // Spines of one kernel variant (fused / full compare / explicit
+      // levels) run together: CTAs of a round work through a few lists at a
+      // time, and mixing variants there thrashes the instruction cache.
+      auto variant = [](const Item& a) {
+        return (a.fused ? 0 : 16) + (a.full ? 0 : 8) + std::min<int>(a.nexp, kMaxExplicit + 1);
+      };
       if (guided)
-        std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) {
-          return a.prio != b.prio ? a.prio < b.prio : a.base < b.base;
+        std::stable_sort(items.begin(), items.end(), [&](const Item& a, const Item& b) {
+          if (a.prio != b.prio) return a.prio < b.prio;
+          if (variant(a) != variant(b)) return variant(a) < variant(b);
+          return a.base < b.base;
         });
       else
-        std::stable_sort(items.begin(), items.end(),
-                         [](const Item& a, const Item& b) { return a.base < b.base; });
+        std::stable_sort(items.begin(), items.end(), [&](const Item& a, const Item& b) {
+          if (variant(a) != variant(b)) return variant(a) < variant(b);
+          return a.base < b.base;
+        });
       for (auto& it : items) {
-        tp.units += it.cblocks * it.vblocks;
+        tp.units += item_units(it);
         tp.cand += (double)it.nctx * (double)it.nv;
         const double w = sizeof(W) == 8 ? 2.0 : 1.0;
         double c = it.full ? w : w + 1.0;
@@ -2180,7 +2398,7 @@ class Batch {
       uint64_t ub = 0;
       for (auto& it : items) {  // unit_begin relative to the list
         it.unit_begin = ub;
-        ub += it.cblocks * it.vblocks;
+        ub += item_units(it);
       }
       TmplDesc td;
       td.item_off = all_items_.size();
@@ -2196,7 +2414,7 @@ class Batch {
         for (int b = 0; b < 64; ++b) {
           tb.item[b] = (unsigned)q;
           tb.unit[b] = uacc;
-          for (; q < items.size() && (int)items[q].prio == b; ++q) uacc += items[q].cblocks * items[q].vblocks;
+          for (; q < items.size() && (int)items[q].prio == b; ++q) uacc += item_units(items[q]);
         }
         tb.item[64] = (unsigned)q;
         tb.unit[64] = uacc;
@@ -2231,7 +2449,7 @@ class Batch {
   std::vector<Task> tasks_;
   std::vector<BuildJob<W>> build_jobs_;
   DevBuf d_tab_, d_smp_, d_cts_, d_best_, d_desc_, d_scal_, d_items_, d_small_, d_ctx_, d_jobs_,
-      d_tasks_, d_tdesc_, d_buckets_, d_mtasks_, d_ns_;
+      d_tasks_, d_tdesc_, d_buckets_, d_mtasks_, d_ns_, d_preq_;
 };
 
 template <class W>

@@ -213,7 +213,7 @@ static int solve_static_typed(const HostInstance& h, int max_size, const EngineO
         if (it.lv[l].kind == 1) it.lv[l].c &= mask;
       finish_item(it, kThreads, mask);
       it.unit_begin = units;
-      units += it.cblocks * it.vblocks;
+      units += item_units(it);
     }
     SB_CUDA(cudaMemcpyAsync(p_items, items.data(), items.size() * sizeof(Item), cudaMemcpyHostToDevice, st));
     // counter = 0, best = ~0, evaluated = 0 (start stamp kept), flags = 0

@@ -49,6 +49,7 @@ def _bind():
                                        P(C.c_float)]
     L.simba_mlp_gradients.argtypes = [C.c_void_p, P(_Instance), C.c_int, P(C.c_int32),
                                       P(C.c_float), P(C.c_float)]
+    L.simba_mlp_apply.argtypes = [C.c_void_p, P(C.c_float), C.c_float]
     L.simba_mlp_predict.argtypes = [C.c_void_p, P(_Instance), C.c_int, P(C.c_float)]
     L.simba_mlp_features.argtypes = [C.c_void_p, P(_Instance), C.c_int, P(C.c_float)]
     L.simba_mlp_get_params.argtypes = [C.c_void_p, P(C.c_float)]
@@ -105,6 +106,14 @@ class Proposal:
                                          C.byref(loss)))
         return g, float(loss.value)
 
+    def apply(self, grads: np.ndarray, lr: float = 1e-3) -> None:
+        """One Adam step with the given gradients (the all-reduced mean in
+        data-parallel training)."""
+        g = np.ascontiguousarray(grads, dtype=np.float32)
+        if g.size != self.n_params:
+            raise ValueError("wrong gradient count")
+        _check(lib().simba_mlp_apply(self._h, _f32p(g), lr))
+
     def predict(self, insts: Sequence[Instance]) -> np.ndarray:
         arrs, ca = _carr(insts)
         p = np.zeros((len(insts), N_CLASSES), dtype=np.float32)
@@ -160,6 +169,47 @@ def train(prop: Proposal, insts: Sequence[Instance], labels: np.ndarray, epochs:
             if len(idx) == 0:
                 continue
             losses.append(prop.train_step([insts[i] for i in idx], labels[idx], lr))
+    return losses
+
+
+def torch_allreduce_mean(group=None):
+    """All-reduce (mean over ranks) of a float32 vector through
+    torch.distributed: NCCL over NVLink for GPU process groups, gloo on CPU."""
+    import torch
+    import torch.distributed as dist
+
+    def reduce(x: np.ndarray) -> np.ndarray:
+        world = dist.get_world_size(group)
+        dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+        t = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float32)).to(dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        return (t / world).cpu().numpy()
+    return reduce
+
+
+def train_dp(prop, insts: Sequence[Instance], labels: np.ndarray, rank: int, world: int,
+             allreduce_mean, epochs: int = 3, batch: int = 256, lr: float = 1e-3,
+             seed: int = 0) -> List[float]:
+    """Data-parallel minibatch Adam: every rank draws the same global
+    minibatch order, computes gradients on its equal share of each
+    minibatch, the shares' gradients are averaged by ``allreduce_mean`` and
+    every rank applies the same Adam step, so the replicas stay identical.
+    With equal shares the mean gradient is the full minibatch's.  Returns
+    the mean loss per step."""
+    rng = np.random.default_rng(seed)
+    n = len(insts)
+    per = batch // world
+    if per == 0:
+        raise ValueError("batch smaller than the number of ranks")
+    losses = []
+    for _ in range(epochs):
+        order = rng.permutation(n)
+        for s in range(0, n - per * world + 1, per * world):  # whole global minibatches only
+            idx = order[s + rank * per: s + (rank + 1) * per]
+            g, loss = prop.gradients([insts[i] for i in idx], labels[idx])
+            g = allreduce_mean(g)
+            losses.append(float(allreduce_mean(np.array([loss], dtype=np.float32))[0]))
+            prop.apply(g, lr)
     return losses
 
 

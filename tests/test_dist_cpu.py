@@ -117,3 +117,79 @@ def test_single_process_loop_without_collective():
     ref = O.search(inst.inputs, inst.outputs, 9, 64)
     assert (res["found"], res["size"], res["rank"], res["candidates"]) == \
         (ref["found"], ref["size"], ref["rank"], ref["candidates"])
+
+
+class OracleProposal:
+    """Stands in for the GPU proposal on CPU: gradients from the numpy
+    oracle of the network (small layer sizes), Adam in numpy; instances
+    are row indices of a fixed feature matrix."""
+
+    DIMS = (32, 16, 16, 8)
+
+    def __init__(self, seed=0):
+        from oracle import mlp_ref as R
+        self.R = R
+        rng = np.random.default_rng(seed)
+        d = self.DIMS
+        n = sum(d[i] * d[i + 1] + d[i + 1] for i in range(3))
+        self.w = (rng.standard_normal(n) * 0.1).astype(np.float32)
+        self.m = np.zeros(n, np.float32)
+        self.v = np.zeros(n, np.float32)
+        self.t = 0
+        self.X = np.sign(np.random.default_rng(99).standard_normal((64, d[0]))).astype(np.float32)
+
+    def gradients(self, rows, labels):
+        loss, g, _ = self.R.forward_backward(self.w, self.X[list(rows)], np.asarray(labels),
+                                             dims=self.DIMS, round_bf16=False)
+        return np.asarray(g, np.float32), float(loss)
+
+    def apply(self, g, lr):
+        self.t += 1
+        b1, b2 = 0.9, 0.999
+        self.m = b1 * self.m + (1 - b1) * g
+        self.v = b2 * self.v + (1 - b2) * g * g
+        mh = self.m / (1 - b1 ** self.t)
+        vh = self.v / (1 - b2 ** self.t)
+        self.w = (self.w - lr * mh / (np.sqrt(vh) + 1e-8)).astype(np.float32)
+
+
+def _dp_worker(rank, world, port, q):
+    import torch.distributed as dist
+    from simba_b200 import guided as G
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        prop = OracleProposal(seed=3)
+        labels = np.arange(64, dtype=np.int32) % 8
+        losses = G.train_dp(prop, list(range(64)), labels, rank, world, G.torch_allreduce_mean(),
+                            epochs=3, batch=16, lr=1e-2)
+        q.put((rank, prop.w, losses))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_data_parallel_training_two_ranks_equals_one():
+    """The proposal's data-parallel training: two gloo ranks, each with half
+    of every minibatch and a mean all-reduce of the gradients, end with the
+    same parameters as one rank training on the whole minibatches."""
+    from simba_b200 import guided as G
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_dp_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = {r: (w, l) for r, w, l in (q.get(timeout=120) for _ in range(2))}
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    one = OracleProposal(seed=3)
+    labels = np.arange(64, dtype=np.int32) % 8
+    ref_losses = G.train_dp(one, list(range(64)), labels, 0, 1, lambda x: x, epochs=3, batch=16,
+                            lr=1e-2)
+    assert np.array_equal(out[0][0], out[1][0])  # replicas stay identical
+    np.testing.assert_allclose(out[0][0], one.w, rtol=1e-4, atol=1e-6)
+    np.testing.assert_allclose(out[0][1], ref_losses, rtol=1e-5)
+    assert ref_losses[-1] < ref_losses[0]

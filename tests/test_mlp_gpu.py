@@ -107,3 +107,17 @@ def test_trained_proposal_beats_uniform_order():
     assert acc > 1.5 / 64  # better than chance
     assert np.median(ratios) < 1.0, (np.median(ratios), acc, len(ratios))
     p.close()
+
+
+def test_apply_equals_train_step():
+    """Gradients + apply (the data-parallel path) is the fused training step."""
+    insts = [make_instance(5 + i % 5, 1 + i % 3, 32, 4400 + i, word_bits=64) for i in range(32)]
+    labels = (np.arange(32) * 7 % 64).astype(np.int32)
+    a, b = G.Proposal(seed=7), G.Proposal(seed=7)
+    la = a.train_step(insts, labels, 1e-3)
+    g, lb = b.gradients(insts, labels)
+    b.apply(g, 1e-3)
+    assert abs(la - lb) < 1e-6
+    assert np.array_equal(a.get_params(), b.get_params())
+    a.close()
+    b.close()
