@@ -76,6 +76,15 @@ constexpr int kPreG = 262144;  // the same queue per CTA in global memory, when 
 constexpr int kR = SIMBA_KR;   // contexts per thread
 constexpr int kMaxExplicit = 2;
 constexpr int kExtra = 3;       // samples besides sample 0 with value tables (match filters)
+// Hash join of fully inverted spines: contexts per block, table slots, bits
+// of the membership filter, bottom values per block, and the fewest contexts
+// for which the join beats the nested compare loop.  Kept small: shared
+// memory taken here is L1 cache lost to every other work unit.
+constexpr int kJoinCtx = 512;
+constexpr int kJoinSlots = 1024;
+constexpr int kJoinBits = 16384;
+constexpr unsigned long long kJoinVals = 1ULL << 18;
+constexpr unsigned long long kJoinMin = 8;
 
 // One level of a spine, top-down (level 0 is the root).
 struct Level {
@@ -227,6 +236,11 @@ struct alignas(16) Smem {
   unsigned long long lk_task_lo, lk_task_hi, lk_item_lo, lk_item_hi;
   int lk_task, lk_item;
   char post[kThreads / 32][kMaxSize + 8];
+  // hash join: membership filter, the block's constraint values and their
+  // context indices
+  unsigned join_bits[kJoinBits / 32];
+  alignas(16) unsigned long long join_key[kJoinSlots];
+  unsigned join_ctx[kJoinSlots];
 };
 
 static_assert(offsetof(Smem, item) % 16 == 0, "Smem::item must be 16-byte aligned");
@@ -752,10 +766,85 @@ __device__ void process_unit_generic(const Params<W>& p, const InstDesc<W>& d, S
   }
 }
 
+// 32-bit mix of a value; its top 14 bits index the filter, the top 10 the table
+__device__ __forceinline__ unsigned join_hash(unsigned long long y) {
+  const unsigned x = (unsigned)y ^ ((unsigned)(y >> 32) * 0x9E3779B1u);
+  return x * 0x85EBCA6Bu;
+}
+
+// A fully inverted spine (no & | * level: every context's constraint is
+// v == K) is a hash join of its contexts with its bottom values: the block's
+// K values go into a shared-memory filter (one bit per hash) and table
+// (linear probing, load <= 1/2), and every bottom value tests the filter and,
+// rarely, probes the table, instead of being compared with each context.  A
+// table hit is an exact sample-0 match and goes to the match queue like any
+// other.
+template <class W, bool FUSED>
+__device__ void process_unit_join(const Params<W>& p, const InstDesc<W>& d, Smem& sm, const Item& it,
+                                  unsigned long long local, const W* s_in, const W* s_out) {
+  static_assert(kJoinBits == 1 << 14 && kJoinSlots == 1 << 10 && kJoinCtx * 2 <= kJoinSlots,
+                "filter and table index widths");
+  const unsigned long long cblk = local / it.vblocks, vblk = local - cblk * it.vblocks;
+  const unsigned long long c0 = cblk * it.cb;
+  const int nc = (int)umin64(it.cb, it.nctx - c0);
+  for (int i = threadIdx.x; i < kJoinSlots; i += blockDim.x) sm.join_ctx[i] = ~0u;
+  for (int i = threadIdx.x; i < kJoinBits / 32; i += blockDim.x) sm.join_bits[i] = 0u;
+  __syncthreads();
+  for (int j = threadIdx.x; j < nc; j += blockDim.x) {
+    W k;
+    if (FUSED) {
+      k = p.ctxs[it.ctx_off + c0 + j].K;
+    } else {
+      W wl[kMaxDepth];
+      decode_context<W>(d, it, c0 + j, wl);
+      W m = (W)~W(0);
+      k = d.target;
+      for (int l = 0; l < it.inv; ++l)
+        if (!invert_level<W>(it.lv[l], wl[l], m, k)) atomicOr(&p.flags[1], 1);
+    }
+    const unsigned hx = join_hash((unsigned long long)k);
+    atomicOr(&sm.join_bits[hx >> 23], 1u << ((hx >> 18) & 31));
+    unsigned h = hx >> 22;
+    for (int t = 0; t < kJoinSlots; ++t, h = (h + 1) & (kJoinSlots - 1)) {
+      if (atomicCAS(&sm.join_ctx[h], ~0u, (unsigned)j) == ~0u) {
+        sm.join_key[h] = (unsigned long long)k;
+        break;
+      }
+    }
+  }
+  __syncthreads();
+  constexpr int VW = 16 / sizeof(W);
+  const W* V = d.tab[it.bottom];
+  const unsigned long long v0 = vblk * it.vb, v1 = umin64(v0 + it.vb, it.nv);
+  const uint4* V4 = reinterpret_cast<const uint4*>(V);
+  for (unsigned long long q = v0 / VW + threadIdx.x; q < (v1 + VW - 1) / VW; q += blockDim.x) {
+    const uint4 raw = __ldg(V4 + q);
+    W xs[VW];
+    memcpy(xs, &raw, 16);
+#pragma unroll
+    for (int e = 0; e < VW; ++e) {
+      const unsigned long long v = q * VW + e;
+      const unsigned long long y = (unsigned long long)xs[e];
+      const unsigned hx = join_hash(y);
+      if (!(sm.join_bits[hx >> 23] >> ((hx >> 18) & 31) & 1u)) continue;
+      unsigned h = hx >> 22;
+      for (int t = 0; t < kJoinSlots; ++t, h = (h + 1) & (kJoinSlots - 1)) {
+        const unsigned c = sm.join_ctx[h];
+        if (c == ~0u) break;
+        if (sm.join_key[h] == y && v >= v0 && v < v1) pre_push<W>(p, d, sm, it, c0 + c, v, s_in, s_out);
+      }
+    }
+  }
+}
+
 template <class W>
 __device__ void dispatch_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm, const Item& it,
                               unsigned long long local, const W* s_in, const W* s_out) {
   const int e = it.nexp;
+  if (it.full == 2) {
+    if (it.fused) return process_unit_join<W, true>(p, d, sm, it, local, s_in, s_out);
+    return process_unit_join<W, false>(p, d, sm, it, local, s_in, s_out);
+  }
   if (it.fused) {
     if (it.full) return process_unit<W, 0, true, true>(p, d, sm, it, local, s_in, s_out);
     return process_unit<W, 0, false, true>(p, d, sm, it, local, s_in, s_out);
@@ -1230,6 +1319,18 @@ static inline void finish_structure(Item& it, uint64_t mask) {
 // bottom values, about 2^22 candidates per unit.
 static inline void finish_layout(Item& it, int threads, uint64_t unit_target = 1ULL << 22) {
   const uint64_t nctx = it.nctx;
+  if (it.full && it.nexp == 0 && nctx >= kJoinMin) {  // hash join (full = 2)
+    it.full = 2;
+    it.G = 0;
+    it.L = 0;
+    it.cb = (uint32_t)std::min<uint64_t>(nctx, kJoinCtx);
+    it.cblocks = (nctx + it.cb - 1) / it.cb;
+    const uint64_t nv_al = (it.nv + 63) / 64 * 64;
+    it.vb = std::min<uint64_t>(nv_al, kJoinVals);
+    it.vblocks = (it.nv + it.vb - 1) / it.vb;
+    it.cpu = 1;
+    return;
+  }
   uint64_t groups = (nctx + kR - 1) / kR;
   int G = 1;
   while (G < threads && (uint64_t)G < groups) G <<= 1;
@@ -1253,6 +1354,23 @@ static inline void finish_layout(Item& it, int threads, uint64_t unit_target = 1
       it.cpu = (uint16_t)std::min<uint64_t>({unit_target / per, it.cblocks, 65535ULL});
     if (it.cpu == 0) it.cpu = 1;
   }
+}
+
+// Integer lane-operations a spine needs.  Nested compares: per candidate
+// the masked compare of the bottom value plus every explicitly evaluated
+// level (64-bit words take two 32-bit lane operations per bitwise or
+// add/sub step and three per multiply).  Hash join: per bottom value and
+// context block the hash and the filter test (5), whatever the number of
+// contexts the block holds.
+static inline double item_alg_ops(const Item& it, size_t wbytes) {
+  const double w = wbytes == 8 ? 2.0 : 1.0;
+  if (it.full == 2) return (double)it.cblocks * (double)it.nv * 5.0;
+  double c = it.full ? w : w + 1.0;
+  for (int l = it.inv; l < it.depth; ++l) {
+    const Level& L = it.lv[l];
+    c += (L.kind == 0 && L.op == OP_MUL) ? (wbytes == 8 ? 3.0 : 1.0) : w;
+  }
+  return (double)it.nctx * (double)it.nv * c;
 }
 
 static inline void finish_item(Item& it, int threads, uint64_t mask) {
@@ -1538,19 +1656,6 @@ class Search final : public SearchSession {
 
   // Search one size; writes the minimum matching rank (or ~0) and the number
   // of candidates evaluated.  status: 0 ok, SIMBA_BUDGET on budget expiry.
-  // Integer lane-operations per candidate that the algorithm needs: the
-  // masked compare of the bottom value plus every explicitly evaluated level
-  // (64-bit words take two 32-bit lane operations per bitwise or add/sub
-  // step and three per multiply).
-  static double alg_cost(const Item& it) {
-    const double w = sizeof(W) == 8 ? 2.0 : 1.0;
-    double c = it.full ? w : w + 1.0;
-    for (int l = it.inv; l < it.depth; ++l) {
-      const Level& L = it.lv[l];
-      c += (L.kind == 0 && L.op == OP_MUL) ? (sizeof(W) == 8 ? 3.0 : 1.0) : w;
-    }
-    return c;
-  }
 
   int search_size(int s, bool stop, uint64_t* best, uint64_t* evaluated, double* ms, int shard = 0,
                   int nshards = 1) {
@@ -1617,7 +1722,7 @@ class Search final : public SearchSession {
       SB_CUDA(d_items_.reserve(items.size() * sizeof(Item)));
       SB_CUDA(cudaMemcpyAsync(d_items_.p, items.data(), items.size() * sizeof(Item),
                               cudaMemcpyHostToDevice, stream_));
-      for (auto& it : items) alg_total += (double)it.nctx * (double)it.nv * alg_cost(it);
+      for (auto& it : items) alg_total += item_alg_ops(it, sizeof(W));
       Params<W> p = params(s);
       p.items = d_items_.as<Item>();
       p.nitems = (int)items.size();
@@ -2373,7 +2478,8 @@ class Batch {
       // levels) run together: CTAs of a round work through a few lists at a
       // time, and mixing variants there thrashes the instruction cache.
       auto variant = [](const Item& a) {
-        return (a.fused ? 0 : 16) + (a.full ? 0 : 8) + std::min<int>(a.nexp, kMaxExplicit + 1);
+        return (a.full == 2 ? 0 : 32) + (a.fused ? 0 : 16) + (a.full ? 0 : 8) +
+               std::min<int>(a.nexp, kMaxExplicit + 1);
       };
       if (guided)
         std::stable_sort(items.begin(), items.end(), [&](const Item& a, const Item& b) {
@@ -2389,11 +2495,7 @@ class Batch {
       for (auto& it : items) {
         tp.units += item_units(it);
         tp.cand += (double)it.nctx * (double)it.nv;
-        const double w = sizeof(W) == 8 ? 2.0 : 1.0;
-        double c = it.full ? w : w + 1.0;
-        for (int l = it.inv; l < it.depth; ++l)
-          c += (it.lv[l].kind == 0 && it.lv[l].op == OP_MUL) ? (sizeof(W) == 8 ? 3.0 : 1.0) : w;
-        tp.alg += (double)it.nctx * (double)it.nv * c;
+        tp.alg += item_alg_ops(it, sizeof(W));
       }
       uint64_t ub = 0;
       for (auto& it : items) {  // unit_begin relative to the list
