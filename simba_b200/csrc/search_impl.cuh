@@ -84,7 +84,7 @@ constexpr int kJoinCtx = 512;
 constexpr int kJoinSlots = 1024;
 constexpr int kJoinBits = 16384;
 constexpr unsigned long long kJoinVals = 1ULL << 18;
-constexpr unsigned long long kJoinMin = 8;
+constexpr unsigned long long kJoinMin = 1;
 
 // One level of a spine, top-down (level 0 is the root).
 struct Level {
@@ -109,7 +109,9 @@ struct alignas(16) Item {
   uint64_t vb;          // bottom values per unit (multiple of 64)
   uint64_t cblocks;     // context blocks
   uint64_t vblocks;     // value blocks
-  uint32_t cb;          // contexts per unit = G * kR
+  uint16_t cb;          // contexts per unit = G * kR (join: per block)
+  int8_t joinable;      // every context's constraint is v & M == K with M a low-bit mask
+  int8_t pad0;
   uint16_t G, L;        // G context groups x L value lanes = kThreads
   int8_t depth, inv, bottom, full, nexp;
   int8_t fused;         // 1: contexts are read from the materialised list
@@ -206,6 +208,7 @@ struct Params {
   int* flags;  // [0] budget expired, [1] inversion failure, [2] queue overflows
   unsigned long long* hits;  // sample-0 matches sent to verification (may be null)
   unsigned long long* preq;  // per-CTA queues of sample-0 matches, [grid][kPreG][2] (may be null)
+  unsigned join_off;         // byte offset of JoinSmem in dynamic shared memory; 0: no join units
   unsigned long long total_units;
   unsigned long long unit_offset;  // this shard's first unit (multi-GPU)
   unsigned long long unit_stride;  // number of shards (0 is read as 1)
@@ -236,11 +239,19 @@ struct alignas(16) Smem {
   unsigned long long lk_task_lo, lk_task_hi, lk_item_lo, lk_item_hi;
   int lk_task, lk_item;
   char post[kThreads / 32][kMaxSize + 8];
-  // hash join: membership filter, the block's constraint values and their
-  // context indices
-  unsigned join_bits[kJoinBits / 32];
-  alignas(16) unsigned long long join_key[kJoinSlots];
-  unsigned join_ctx[kJoinSlots];
+};
+
+// Hash join tables of a CTA: membership filter, the block's constraint
+// values, their context indices and mask widths.  They sit after the
+// staged samples in the dynamic shared memory of the launches that run
+// join units only (Params::join_off), so that the other launches keep
+// their shared memory, and L1 cache, as they were.
+struct alignas(16) JoinSmem {
+  unsigned long long key[kJoinSlots];
+  unsigned ctx[kJoinSlots];
+  unsigned bits[kJoinBits / 32];
+  unsigned char b[kJoinSlots];  // low-bit mask width of the slot's constraint
+  unsigned long long mc;        // AND of the block's masks: the bits joined on
 };
 
 static_assert(offsetof(Smem, item) % 16 == 0, "Smem::item must be 16-byte aligned");
@@ -772,47 +783,77 @@ __device__ __forceinline__ unsigned join_hash(unsigned long long y) {
   return x * 0x85EBCA6Bu;
 }
 
-// A fully inverted spine (no & | * level: every context's constraint is
-// v == K) is a hash join of its contexts with its bottom values: the block's
-// K values go into a shared-memory filter (one bit per hash) and table
-// (linear probing, load <= 1/2), and every bottom value tests the filter and,
-// rarely, probes the table, instead of being compared with each context.  A
-// table hit is an exact sample-0 match and goes to the match queue like any
-// other.
+// A spine without & and | levels inverts every context to v & M == K with M
+// a low-bit mask (all ones unless a * level's small value is even), so
+// matching a block of contexts against all bottom values is a hash join on
+// the low bits Mc that all the block's masks keep: the contexts' K & Mc go
+// into a shared-memory filter (one bit per hash) and table (linear probing,
+// load <= 1/2), every bottom value tests the filter with v & Mc and, rarely,
+// probes the table, and a table entry matches when v & M == K for its own
+// mask.  A block with a context of a narrow mask (a small value 0 makes
+// M = 0) joins on few bits and probes long chains: slower, still exact.  A
+// match is an exact sample-0 match and goes to the match queue like any
+// other; contexts whose K has bits outside M can never match and are left
+// out.
 template <class W, bool FUSED>
-__device__ void process_unit_join(const Params<W>& p, const InstDesc<W>& d, Smem& sm, const Item& it,
-                                  unsigned long long local, const W* s_in, const W* s_out) {
+__device__ void process_unit_join(const Params<W>& p, const InstDesc<W>& d, Smem& sm, JoinSmem& js,
+                                  const Item& it, unsigned long long local, const W* s_in,
+                                  const W* s_out) {
   static_assert(kJoinBits == 1 << 14 && kJoinSlots == 1 << 10 && kJoinCtx * 2 <= kJoinSlots,
                 "filter and table index widths");
+  static_assert(kJoinCtx <= 2 * kThreads, "two contexts per thread at most");
+  constexpr int WB = 8 * (int)sizeof(W);
   const unsigned long long cblk = local / it.vblocks, vblk = local - cblk * it.vblocks;
   const unsigned long long c0 = cblk * it.cb;
   const int nc = (int)umin64(it.cb, it.nctx - c0);
-  for (int i = threadIdx.x; i < kJoinSlots; i += blockDim.x) sm.join_ctx[i] = ~0u;
-  for (int i = threadIdx.x; i < kJoinBits / 32; i += blockDim.x) sm.join_bits[i] = 0u;
+  for (int i = threadIdx.x; i < kJoinSlots; i += blockDim.x) js.ctx[i] = ~0u;
+  for (int i = threadIdx.x; i < kJoinBits / 32; i += blockDim.x) js.bits[i] = 0u;
+  if (threadIdx.x == 0) js.mc = ~0ULL;
   __syncthreads();
-  for (int j = threadIdx.x; j < nc; j += blockDim.x) {
-    W k;
+  // 1. constraints of this thread's (at most two) contexts; the common mask
+  W ms[2], ks[2];
+  bool ok[2];
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int j = threadIdx.x + r * blockDim.x;
+    ok[r] = false;
+    if (j >= nc) continue;
+    W m = (W)~W(0), k = d.target;
     if (FUSED) {
-      k = p.ctxs[it.ctx_off + c0 + j].K;
+      const Ctx<W> cx = p.ctxs[it.ctx_off + c0 + j];
+      m = cx.M;
+      k = cx.K;
     } else {
       W wl[kMaxDepth];
       decode_context<W>(d, it, c0 + j, wl);
-      W m = (W)~W(0);
-      k = d.target;
       for (int l = 0; l < it.inv; ++l)
         if (!invert_level<W>(it.lv[l], wl[l], m, k)) atomicOr(&p.flags[1], 1);
     }
-    const unsigned hx = join_hash((unsigned long long)k);
-    atomicOr(&sm.join_bits[hx >> 23], 1u << ((hx >> 18) & 31));
+    ms[r] = m;
+    ks[r] = k;
+    ok[r] = (W)(k & ~m) == 0;  // otherwise no bottom value can match
+    if (ok[r]) atomicAnd(&js.mc, (unsigned long long)m);
+  }
+  __syncthreads();
+  const unsigned long long mc = js.mc;
+  // 2. filter bits and table entries, keyed on K & Mc
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    if (!ok[r]) continue;
+    const int j = threadIdx.x + r * blockDim.x;
+    const unsigned hx = join_hash((unsigned long long)ks[r] & mc);
+    atomicOr(&js.bits[hx >> 23], 1u << ((hx >> 18) & 31));
     unsigned h = hx >> 22;
     for (int t = 0; t < kJoinSlots; ++t, h = (h + 1) & (kJoinSlots - 1)) {
-      if (atomicCAS(&sm.join_ctx[h], ~0u, (unsigned)j) == ~0u) {
-        sm.join_key[h] = (unsigned long long)k;
+      if (atomicCAS(&js.ctx[h], ~0u, (unsigned)j) == ~0u) {
+        js.key[h] = (unsigned long long)ks[r];
+        js.b[h] = (unsigned char)__popcll((unsigned long long)ms[r]);
         break;
       }
     }
   }
   __syncthreads();
+  // 3. probe with every bottom value of the block
   constexpr int VW = 16 / sizeof(W);
   const W* V = d.tab[it.bottom];
   const unsigned long long v0 = vblk * it.vb, v1 = umin64(v0 + it.vb, it.nv);
@@ -825,25 +866,35 @@ __device__ void process_unit_join(const Params<W>& p, const InstDesc<W>& d, Smem
     for (int e = 0; e < VW; ++e) {
       const unsigned long long v = q * VW + e;
       const unsigned long long y = (unsigned long long)xs[e];
-      const unsigned hx = join_hash(y);
-      if (!(sm.join_bits[hx >> 23] >> ((hx >> 18) & 31) & 1u)) continue;
+      const unsigned long long ym = y & mc;
+      const unsigned hx = join_hash(ym);
+      if (!(js.bits[hx >> 23] >> ((hx >> 18) & 31) & 1u)) continue;
       unsigned h = hx >> 22;
       for (int t = 0; t < kJoinSlots; ++t, h = (h + 1) & (kJoinSlots - 1)) {
-        const unsigned c = sm.join_ctx[h];
+        const unsigned c = js.ctx[h];
         if (c == ~0u) break;
-        if (sm.join_key[h] == y && v >= v0 && v < v1) pre_push<W>(p, d, sm, it, c0 + c, v, s_in, s_out);
+        const unsigned long long key = js.key[h];
+        if ((key & mc) != ym) continue;
+        const int b = js.b[h];
+        const unsigned long long m = b >= WB ? (unsigned long long)(W)~W(0) : ((1ULL << b) - 1);
+        if ((y & m) == key && v >= v0 && v < v1) pre_push<W>(p, d, sm, it, c0 + c, v, s_in, s_out);
       }
     }
   }
 }
 
 template <class W>
-__device__ void dispatch_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm, const Item& it,
-                              unsigned long long local, const W* s_in, const W* s_out) {
+__device__ void dispatch_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm, JoinSmem* js,
+                              const Item& it, unsigned long long local, const W* s_in,
+                              const W* s_out) {
   const int e = it.nexp;
   if (it.full == 2) {
-    if (it.fused) return process_unit_join<W, true>(p, d, sm, it, local, s_in, s_out);
-    return process_unit_join<W, false>(p, d, sm, it, local, s_in, s_out);
+    if (!js) {  // a join unit in a launch without join tables: host error
+      if (threadIdx.x == 0) atomicOr(&p.flags[1], 2);
+      return;
+    }
+    if (it.fused) return process_unit_join<W, true>(p, d, sm, *js, it, local, s_in, s_out);
+    return process_unit_join<W, false>(p, d, sm, *js, it, local, s_in, s_out);
   }
   if (it.fused) {
     if (it.full) return process_unit<W, 0, true, true>(p, d, sm, it, local, s_in, s_out);
@@ -902,6 +953,7 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
   W* s_in = reinterpret_cast<W*>(smem_raw + ((sizeof(Smem) + 15) & ~size_t(15)));
   W* s_out = s_in;
+  JoinSmem* js = p.join_off ? reinterpret_cast<JoinSmem*>(smem_raw + p.join_off) : nullptr;
   const InstDesc<W>& d = *reinterpret_cast<const InstDesc<W>*>(sm.desc);
   if (threadIdx.x == 0) {
     sm.qn = 0;
@@ -1012,7 +1064,7 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
       const unsigned long long cpu = it.cpu ? it.cpu : 1;
       const unsigned long long b0 = cu * cpu, b1 = umin64(b0 + cpu, it.cblocks);
       for (unsigned long long b = b0; b < b1; ++b) {
-        dispatch_unit<W>(p, d, sm, it, b * it.vblocks + vblk, s_in, s_out);
+        dispatch_unit<W>(p, d, sm, js, it, b * it.vblocks + vblk, s_in, s_out);
         if (threadIdx.x == 0) {
           const unsigned long long c0 = b * it.cb, c1 = umin64(c0 + it.cb, it.nctx);
           const unsigned long long v0 = vblk * it.vb, v1 = umin64(v0 + it.vb, it.nv);
@@ -1309,6 +1361,9 @@ static inline void finish_structure(Item& it, uint64_t mask) {
   it.inv = (int8_t)inv;
   it.nexp = (int8_t)(it.depth - inv);
   it.full = full ? 1 : 0;
+  // without & and |, inversion only ever narrows the mask to the low bits
+  // (at * levels), so the spine can be joined on those bits
+  it.joinable = (!andor && it.nexp == 0) ? 1 : 0;
   uint64_t nctx = 1;
   for (int l = 0; l < it.depth; ++l)
     if (it.lv[l].kind == 0) nctx *= it.lv[l].nsmall;
@@ -1319,7 +1374,7 @@ static inline void finish_structure(Item& it, uint64_t mask) {
 // bottom values, about 2^22 candidates per unit.
 static inline void finish_layout(Item& it, int threads, uint64_t unit_target = 1ULL << 22) {
   const uint64_t nctx = it.nctx;
-  if (it.full && it.nexp == 0 && nctx >= kJoinMin) {  // hash join (full = 2)
+  if (it.joinable && nctx >= kJoinMin) {  // hash join (full = 2)
     it.full = 2;
     it.G = 0;
     it.L = 0;
@@ -1425,6 +1480,7 @@ static inline void fuse_small(std::vector<Item>& items, std::vector<Item>* small
     size_t gi = 0;
     for (; gi < groups.size(); ++gi)
       if (groups[gi].bottom == it.bottom && groups[gi].full == it.full &&
+          groups[gi].joinable == it.joinable &&
           (!by_prio || groups[gi].prio == it.prio))
         break;
     if (gi == groups.size()) {
@@ -1432,6 +1488,7 @@ static inline void fuse_small(std::vector<Item>& items, std::vector<Item>* small
       memset(&g, 0, sizeof(g));
       g.bottom = it.bottom;
       g.full = it.full;
+      g.joinable = it.joinable;
       g.prio = it.prio;
       g.fused = 1;
       g.nv = ct.n[(int)it.bottom][8];
@@ -1459,6 +1516,17 @@ static inline void fuse_small(std::vector<Item>& items, std::vector<Item>* small
             [](const Item& a, const Item& b) { return a.ctx_off < b.ctx_off; });
   *nctxs = off;
   items.swap(keep);
+}
+
+// Raise (never lower) a kernel's dynamic shared memory limit: sessions,
+// batches and the static entry point share the kernel functions, and a
+// lower limit set by one would make another's launches fail.
+static inline cudaError_t raise_smem_limit(const void* f, size_t bytes) {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, f);
+  if (e != cudaSuccess) return e;
+  if ((size_t)a.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+  return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 template <class W>
@@ -1524,14 +1592,17 @@ class Search final : public SearchSession {
     built_ = 0;
     smem_bytes_ = ((sizeof(Smem) + 15) & ~size_t(15)) +
                   (((size_t)h_.S * h_.k * sizeof(W) + 15) / 16 + ((size_t)h_.S * sizeof(W) + 15) / 16) * 16;
-    SB_CUDA(cudaFuncSetAttribute(spine_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem_bytes_));
-    SB_CUDA(cudaFuncSetAttribute(naive_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem_bytes_));
+    join_off_ = (smem_bytes_ + 15) & ~size_t(15);  // join launches: tables after the samples
+    smem_join_ = join_off_ + sizeof(JoinSmem);
+    SB_CUDA(raise_smem_limit((const void*)spine_kernel<W>, smem_join_));
+    SB_CUDA(raise_smem_limit((const void*)naive_kernel<W>, smem_bytes_));
     int occ = 1;
     SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, spine_kernel<W>, kThreads, smem_bytes_));
     grid_ = sms_ * std::max(occ, 1);
-    SB_CUDA(d_preq_.reserve((size_t)grid_ * kPreG * 16));
+    int occj = 1;
+    SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occj, spine_kernel<W>, kThreads, smem_join_));
+    grid_join_ = sms_ * std::max(occj, 1);
+    SB_CUDA(d_preq_.reserve((size_t)std::max(grid_, grid_join_) * kPreG * 16));
     int occn = 1;
     SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occn, naive_kernel<W>, kThreads, smem_bytes_));
     grid_naive_ = sms_ * std::max(occn, 1);
@@ -1714,18 +1785,31 @@ class Search final : public SearchSession {
       else
         std::stable_sort(items.begin(), items.end(),
                          [](const Item& a, const Item& b) { return a.base < b.base; });
-      uint64_t units = 0;
-      for (auto& it : items) {
-        it.unit_begin = units;
-        units += item_units(it);
+      // join units run in a launch of their own (with the join tables in
+      // shared memory), the nested-compare units in another
+      std::stable_partition(items.begin(), items.end(), [](const Item& a) { return a.full == 2; });
+      size_t nj = 0;
+      while (nj < items.size() && items[nj].full == 2) ++nj;
+      uint64_t units = 0, units_join = 0;
+      for (size_t q = 0; q < items.size(); ++q) {
+        if (q == nj) {
+          units_join = units;
+          units = 0;
+        }
+        items[q].unit_begin = units;
+        units += item_units(items[q]);
+      }
+      if (nj == items.size()) {
+        units_join = units;
+        units = 0;
       }
       SB_CUDA(d_items_.reserve(items.size() * sizeof(Item)));
       SB_CUDA(cudaMemcpyAsync(d_items_.p, items.data(), items.size() * sizeof(Item),
                               cudaMemcpyHostToDevice, stream_));
       for (auto& it : items) alg_total += item_alg_ops(it, sizeof(W));
       Params<W> p = params(s);
-      p.items = d_items_.as<Item>();
-      p.nitems = (int)items.size();
+      p.items = d_items_.as<Item>() + nj;
+      p.nitems = (int)(items.size() - nj);
       p.total_units = units;
       p.unit_offset = (unsigned long long)shard;
       p.unit_stride = (unsigned long long)nshards;
@@ -1744,8 +1828,20 @@ class Search final : public SearchSession {
         ++launches_;
         p.ctxs = d_ctx_.as<Ctx<W>>();
       }
-      spine_kernel<W><<<grid_, kThreads, smem_bytes_, stream_>>>(p);
-      ++launches_;
+      if (nj) {
+        Params<W> pj = p;
+        pj.items = d_items_.as<Item>();
+        pj.nitems = (int)nj;
+        pj.total_units = units_join;
+        pj.join_off = (unsigned)join_off_;
+        spine_kernel<W><<<grid_join_, kThreads, smem_join_, stream_>>>(pj);
+        ++launches_;
+      }
+      if (nj < items.size()) {
+        p.counter = d_scal_.as<unsigned long long>() + 7;  // zeroed with the flags
+        spine_kernel<W><<<grid_, kThreads, smem_bytes_, stream_>>>(p);
+        ++launches_;
+      }
       SB_CUDA(cudaGetLastError());
     } else {
       Params<W> p = params(s);
@@ -1882,8 +1978,8 @@ class Search final : public SearchSession {
   int launches_ = 0;
   double kernel_ms_ = 0.0;
   uint64_t alg_ops_ = 0;
-  int sms_ = 0, grid_ = 0, grid_naive_ = 0;
-  size_t smem_bytes_ = 0;
+  int sms_ = 0, grid_ = 0, grid_naive_ = 0, grid_join_ = 0;
+  size_t smem_bytes_ = 0, join_off_ = 0, smem_join_ = 0;
   DevBuf d_in_, d_out_, d_counts_, d_scal_, d_items_, d_small_, d_ctx_, d_insts_, d_preq_;
   DevBuf d_tabs_[kMaxSize + 1];  // V_t of every sample, allocated when size t is first built
   unsigned long long h_scal_[8] = {};
@@ -2062,10 +2158,12 @@ class Batch {
                                         toff[i][t]);
     };
     auto next_cost = [&](int i) { return swept[i] + (double)cts_[ct_of[i]].n[size[i]][8]; };
-    const size_t smem = ((sizeof(Smem) + 15) & ~size_t(15)) +
-                        (((size_t)maxS * maxK * sizeof(W) + 15) / 16 + ((size_t)maxS * sizeof(W) + 15) / 16) * 16;
-    SB_CUDA(cudaFuncSetAttribute(spine_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    SB_CUDA(cudaFuncSetAttribute(naive_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t smem_base = ((sizeof(Smem) + 15) & ~size_t(15)) +
+                             (((size_t)maxS * maxK * sizeof(W) + 15) / 16 + ((size_t)maxS * sizeof(W) + 15) / 16) * 16;
+    const size_t join_off = (smem_base + 15) & ~size_t(15);  // one launch: join tables included
+    const size_t smem = join_off + sizeof(JoinSmem);
+    SB_CUDA(raise_smem_limit((const void*)spine_kernel<W>, smem));
+    SB_CUDA(raise_smem_limit((const void*)naive_kernel<W>, smem));
     int occ = 1;
     SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, spine_kernel<W>, kThreads, smem));
     const int grid = sms * std::max(occ, 1);
@@ -2281,6 +2379,7 @@ class Batch {
       p.flags = reinterpret_cast<int*>(sc + 4);
       p.hits = sc + 6;
       p.preq = d_preq_.as<unsigned long long>();
+      p.join_off = (unsigned)join_off;
       p.maxS = maxS;
       p.maxK = maxK;
       p.stop_on_match = guided ? 2 : 1;  // guided: any verified match of the size

@@ -130,8 +130,10 @@ static int solve_static_typed(const HostInstance& h, int max_size, const EngineO
     }
   int sms = 0;
   SB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, o.device));
-  const size_t smem = ((sizeof(Smem) + 15) & ~size_t(15)) + (nin16 + nout16) * 16;
-  SB_CUDA(cudaFuncSetAttribute(spine_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const size_t smem_base = ((sizeof(Smem) + 15) & ~size_t(15)) + (nin16 + nout16) * 16;
+  const size_t join_off = (smem_base + 15) & ~size_t(15);  // one launch: join tables included
+  const size_t smem = join_off + sizeof(JoinSmem);
+  SB_CUDA(raise_smem_limit((const void*)spine_kernel<W>, smem));
   int occ = 1;
   SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, spine_kernel<W>, kThreads, smem));
   const int grid = sms * std::max(occ, 1);
@@ -246,6 +248,7 @@ static int solve_static_typed(const HostInstance& h, int max_size, const EngineO
     p.nitems = (int)items.size();
     p.total_units = units;
     p.stop_on_match = 1;
+    p.join_off = (unsigned)join_off;
     spine_kernel<W><<<grid, kThreads, smem, st>>>(p);
     ++out->launches;
     SB_CUDA(cudaGetLastError());
