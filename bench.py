@@ -12,9 +12,10 @@ value     candidates / second with samples and value tables resident in HBM
           (session API), timed with CUDA events on the launching stream.
 e2e       the same metric through simba_solve() from host buffers: H2D of the
           samples, table build, search, D2H of the result, every step.
-roofline  the search kernel's integer lane-operations (the masked compare
-          and explicitly evaluated levels per candidate) over the measured
-          int32 issue peak of the device (simba_int_peak).
+roofline  the search kernel's integer lane-operations (nested compares: the
+          masked compare and explicitly evaluated levels per candidate; hash
+          join: hash and filter test per bottom value and context block) over
+          the measured int32 issue peak of the device (simba_int_peak).
 cpu_baseline  the OpenMP oracle (a port of the reference's per-rank
           unrank + evaluate) on a bounded sample of size-L ranks.
 
@@ -233,7 +234,7 @@ def run_ours(a, rank: int, world: int, local_rank: int) -> None:
                                    "unsatisfiable target (the size-15 config with its outputs "
                                    "randomised so every block is searched)",
                        "candidates_per_step": cand_step, "engine": "tabled spine kernel",
-                       "l2": "inputs larger than L2 (value tables up to 1.3 GB)",
+                       "l2": "inputs larger than L2 (value tables of 4 samples up to 5.8 GB)",
                        "parallelism": f"independent instances x{world}"},
             "e2e": e2e,
             "roofline": {"bound": "int-alu", "achieved": achieved / 1e12, "peak": peak / 1e12,

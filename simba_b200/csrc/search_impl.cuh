@@ -803,7 +803,9 @@ __device__ void process_unit_join(const Params<W>& p, const InstDesc<W>& d, Smem
                 "filter and table index widths");
   static_assert(kJoinCtx <= 2 * kThreads, "two contexts per thread at most");
   constexpr int WB = 8 * (int)sizeof(W);
-  const unsigned long long cblk = local / it.vblocks, vblk = local - cblk * it.vblocks;
+  // value-block major: consecutive units (on other CTAs) share a value
+  // block, which then comes from L2 for every context block after the first
+  const unsigned long long vblk = local / it.cblocks, cblk = local - vblk * it.cblocks;
   const unsigned long long c0 = cblk * it.cb;
   const int nc = (int)umin64(it.cb, it.nctx - c0);
   for (int i = threadIdx.x; i < kJoinSlots; i += blockDim.x) js.ctx[i] = ~0u;
@@ -858,8 +860,7 @@ __device__ void process_unit_join(const Params<W>& p, const InstDesc<W>& d, Smem
   const W* V = d.tab[it.bottom];
   const unsigned long long v0 = vblk * it.vb, v1 = umin64(v0 + it.vb, it.nv);
   const uint4* V4 = reinterpret_cast<const uint4*>(V);
-  for (unsigned long long q = v0 / VW + threadIdx.x; q < (v1 + VW - 1) / VW; q += blockDim.x) {
-    const uint4 raw = __ldg(V4 + q);
+  auto probe = [&](const uint4& raw, unsigned long long q) {
     W xs[VW];
     memcpy(xs, &raw, 16);
 #pragma unroll
@@ -880,7 +881,21 @@ __device__ void process_unit_join(const Params<W>& p, const InstDesc<W>& d, Smem
         if ((y & m) == key && v >= v0 && v < v1) pre_push<W>(p, d, sm, it, c0 + c, v, s_in, s_out);
       }
     }
+  };
+  // four 16-byte loads in flight per thread
+  const unsigned long long q1 = (v1 + VW - 1) / VW, step = blockDim.x;
+  unsigned long long q = v0 / VW + threadIdx.x;
+  for (; q + 3 * step < q1; q += 4 * step) {
+    const uint4 a0 = __ldg(V4 + q);
+    const uint4 a1 = __ldg(V4 + q + step);
+    const uint4 a2 = __ldg(V4 + q + 2 * step);
+    const uint4 a3 = __ldg(V4 + q + 3 * step);
+    probe(a0, q);
+    probe(a1, q + step);
+    probe(a2, q + 2 * step);
+    probe(a3, q + 3 * step);
   }
+  for (; q < q1; q += step) probe(__ldg(V4 + q), q);
 }
 
 template <class W>
@@ -1060,11 +1075,16 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
         if (threadIdx.x == 0) sm.inst_idx = (int)it.inst;
       }
       const unsigned long long local = sm.unit_local;
-      const unsigned long long cu = local / it.vblocks, vblk = local - cu * it.vblocks;
+      unsigned long long cu = local / it.vblocks, vblk = local - cu * it.vblocks;
+      if (it.full == 2) {  // join units are value-block major (cpu = 1)
+        vblk = local / it.cblocks;
+        cu = local - vblk * it.cblocks;
+      }
       const unsigned long long cpu = it.cpu ? it.cpu : 1;
       const unsigned long long b0 = cu * cpu, b1 = umin64(b0 + cpu, it.cblocks);
       for (unsigned long long b = b0; b < b1; ++b) {
-        dispatch_unit<W>(p, d, sm, js, it, b * it.vblocks + vblk, s_in, s_out);
+        const unsigned long long lb = it.full == 2 ? vblk * it.cblocks + b : b * it.vblocks + vblk;
+        dispatch_unit<W>(p, d, sm, js, it, lb, s_in, s_out);
         if (threadIdx.x == 0) {
           const unsigned long long c0 = b * it.cb, c1 = umin64(c0 + it.cb, it.nctx);
           const unsigned long long v0 = vblk * it.vb, v1 = umin64(v0 + it.vb, it.nv);
