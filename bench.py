@@ -57,7 +57,33 @@ def parse():
     ap.add_argument("--sweep", type=int, default=SWEEP_L)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--case", choices=["spine12", "batch10", "vfb10"],
+                    help="run one small profiling case instead of the benchmark (no JSON line)")
     return ap.parse_args()
+
+
+def run_case(name: str) -> None:
+    """Small cases for ncu captures (see profiles/): a size-12 sweep of the
+    benchmark instance run twice; a 256-instance mixed batch to max size 11
+    (its 9th spine launch is the size-10 round); VFB to maxLen 10 on the
+    benchmark instance."""
+    sys.path.insert(0, str(ROOT))
+    import simba_b200 as S
+    from simba_b200.instances import iter_batch, make_instance
+    inst = make_instance(TARGET_SIZE, N_VARS, N_SAMPLES, 1, word_bits=64, unsat=True)
+    if name == "spine12":
+        with S.Session(inst) as ss:
+            for _ in range(2):
+                r = ss.sweep(12, 12)
+        print("spine12", r.candidates, r.evaluated, r.kernel_ms)
+    elif name == "batch10":
+        insts = list(iter_batch(256, 5 * 10 ** 6, sizes=range(7, 20), vars_=(2, 3, 4, 5),
+                                samples=(32, 64, 128), word_bits=64))
+        res, st = S.solve_batch(insts, 11, table_bytes=12 << 20, budget=60)
+        print("batch10", st["rounds"], st["evaluated"], st["kernel_ms"], st["solved"])
+    else:
+        r = S.vfb_solve(inst, 10, budget=120)
+        print("vfb10", r.status, r.candidates, r.rows_total, r.device_ms)
 
 
 class Clocks:
@@ -313,6 +339,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.case:
+        run_case(a.case)
+        return
     if a.impl == "reference":
         run_reference(a, rank)
         return
