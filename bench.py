@@ -220,13 +220,14 @@ def run_ours(a, rank: int, world: int, local_rank: int) -> None:
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
+        S.solve(inst, L + 1, device=local_rank)  # warm-up: module loading, allocator
         times = []
         for i in range(max(1, min(a.steps, 3))):
             t0 = time.perf_counter()
             rr = S.solve(inst, L + 1, device=local_rank)
             times.append(time.perf_counter() - t0)
             assert rr.status == S.NOT_FOUND and rr.candidates == cand_step
-        el = max(times) if False else statistics.mean(times)
+        el = statistics.mean(times)
         if dist:
             t = torch.tensor([el], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)

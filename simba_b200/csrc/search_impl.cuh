@@ -1597,17 +1597,25 @@ class Search final : public SearchSession {
 
     // table budget -> largest tabled size
     const int64_t budget = o_.table_bytes > 0 ? o_.table_bytes : (8LL << 30);
-    uint64_t total = 0;
     Tcap_ = 0;
-    // every tabled size has the tables of all samples (sample 0 and the
-    // filter samples): a spine touching a size without filter tables would
-    // send its sparse-mask matches to verification unfiltered
+    // The filter samples' tables take at most an eighth of the budget
+    // (sizes up to Tf_): a single search has large tables and few sparse-
+    // mask matches, and building four copies of the largest size would
+    // dominate a solve from host buffers.  A spine that needs a table above
+    // Tf_ sends its sample-0 matches to verification unfiltered.
+    uint64_t cum0 = 0, cumf = 0;
+    Tf_ = 0;
     for (int t = 1; t <= count_ok_max_ && t <= 20; ++t) {
-      const uint64_t bytes = padded(ct_.n[t][8]) * sizeof(W) * nsamp();
-      if (total + bytes > (uint64_t)budget) break;
-      total += bytes;
+      const uint64_t bytes = padded(ct_.n[t][8]) * sizeof(W);
+      if (nsamp() > 1 && (cum0 + bytes) * (nsamp() - 1) <= (uint64_t)budget / 8 && Tf_ == t - 1) {
+        Tf_ = t;
+        cumf = (cum0 + bytes) * (nsamp() - 1);
+      }
+      if (cum0 + bytes + cumf > (uint64_t)budget) break;
+      cum0 += bytes;
       Tcap_ = t;
     }
+    if (Tf_ > Tcap_) Tf_ = Tcap_;
     if (Tcap_ < 1) Tcap_ = 1;  // tables are allocated when first built
     built_ = 0;
     smem_bytes_ = ((sizeof(Smem) + 15) & ~size_t(15)) +
@@ -1669,8 +1677,9 @@ class Search final : public SearchSession {
   // Build V_{built+1} .. V_t (each entry one operator over smaller tables).
   int ensure_tables(int t) {
     for (int s = built_ + 1; s <= t; ++s) {
-      SB_CUDA(d_tabs_[s].reserve(padded(ct_.n[s][8]) * sizeof(W) * nsamp()));
-      for (int j = 0; j < nsamp(); ++j) {
+      const int copies = s <= Tf_ ? nsamp() : 1;
+      SB_CUDA(d_tabs_[s].reserve(padded(ct_.n[s][8]) * sizeof(W) * copies));
+      for (int j = 0; j < copies; ++j) {
         W* o = tab(s, j);
         if (s == 1) {
           std::vector<W> v(padded(h_.k), 0);
@@ -1713,7 +1722,8 @@ class Search final : public SearchSession {
     memset(&d, 0, sizeof(d));
     for (int t = 1; t <= built_; ++t) {
       d.tab[t] = tab(t);
-      for (int j = 1; j < nsamp(); ++j) d.tabx[j - 1][t] = tab(t, j);
+      if (t <= Tf_)
+        for (int j = 1; j < nsamp(); ++j) d.tabx[j - 1][t] = tab(t, j);
     }
     for (int j = 1; j < nsamp(); ++j) d.targetx[j - 1] = (W)h_.out[j];
     d.in = d_in_.as<W>();
@@ -2003,7 +2013,7 @@ class Search final : public SearchSession {
   DevBuf d_in_, d_out_, d_counts_, d_scal_, d_items_, d_small_, d_ctx_, d_insts_, d_preq_;
   DevBuf d_tabs_[kMaxSize + 1];  // V_t of every sample, allocated when size t is first built
   unsigned long long h_scal_[8] = {};
-  int Tcap_ = 0, built_ = 0, last_T_ = 0;
+  int Tcap_ = 0, Tf_ = 0, built_ = 0, last_T_ = 0;
 };
 
 // ------------------------------------------------------------------ batch
