@@ -83,7 +83,7 @@ constexpr int kExtra = 3;       // samples besides sample 0 with value tables (m
 constexpr int kJoinCtx = 512;
 constexpr int kJoinSlots = 1024;
 constexpr int kJoinBits = 16384;
-constexpr unsigned long long kJoinVals = 1ULL << 18;
+constexpr unsigned long long kJoinVals = 1ULL << 15;
 constexpr unsigned long long kJoinMin = 1;
 
 // One level of a spine, top-down (level 0 is the root).

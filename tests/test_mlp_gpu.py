@@ -117,7 +117,8 @@ def test_apply_equals_train_step():
     la = a.train_step(insts, labels, 1e-3)
     g, lb = b.gradients(insts, labels)
     b.apply(g, 1e-3)
-    assert abs(la - lb) < 1e-6
-    assert np.array_equal(a.get_params(), b.get_params())
+    # the loss is summed over rows with atomics, in no fixed order
+    assert abs(la - lb) <= 1e-5 * max(1.0, abs(la))
+    np.testing.assert_allclose(a.get_params(), b.get_params(), rtol=1e-5, atol=1e-6)
     a.close()
     b.close()
