@@ -64,27 +64,28 @@ class SplitMix64:
                 return x % n
 
 
-def random_postfix(size: int, n_terms: int, rng: SplitMix64) -> str:
+def random_postfix(size: int, n_terms: int, rng: SplitMix64,
+                   binary: Sequence[str] = ("-", "+", "*", "&", "|", "^")) -> str:
     """Random expression of exactly ``size`` nodes, as a postfix string.
 
     Terminals are written ``'0' + t`` and operators with the reference's
     characters, which is the encoding of ``numberToFormula``
-    (simba/src/nocache.cu:44-45,60).
+    (simba/src/nocache.cu:44-45,60).  ``binary`` restricts the binary
+    operators drawn (default: all six, the generator's distribution).
     """
     if size < 1:
         raise ValueError("size must be >= 1")
     if size == 1:
         return chr(ord("0") + rng.below(n_terms))
     unary = ["#", "~"]
-    binary = ["-", "+", "*", "&", "|", "^"]
-    allowed = unary + (binary if size >= 3 else [])
+    allowed = unary + (list(binary) if size >= 3 else [])
     op = allowed[rng.below(len(allowed))]
     if op in UNARY:
-        return random_postfix(size - 1, n_terms, rng) + op
+        return random_postfix(size - 1, n_terms, rng, binary) + op
     left = 1 + rng.below(size - 2)
     right = size - 1 - left
-    return (random_postfix(left, n_terms, rng)
-            + random_postfix(right, n_terms, rng) + op)
+    return (random_postfix(left, n_terms, rng, binary)
+            + random_postfix(right, n_terms, rng, binary) + op)
 
 
 def eval_postfix(postfix: str, inputs: np.ndarray, word_bits: int) -> np.ndarray:
@@ -298,6 +299,27 @@ def make_instance(size: int, n_vars: int, n_samples: int, seed: int,
         outs = np.array([rng.next() & mask for _ in range(n_samples)], dtype=np.uint64)
     return Instance(n_terms, ins, outs, word_bits, None if unsat else formula,
                     const_one, {"size": size, "seed": seed, "unsat": unsat})
+
+
+def planted_instance(postfix: str, n_vars: int, n_samples: int, seed: int,
+                     word_bits: int = 64, const_one: bool = True) -> Instance:
+    """Instance whose outputs are the given expression evaluated on seeded
+    uniform random samples (SplitMix64(seed)), ``n_vars`` variables plus the
+    constant 1 when ``const_one``.  The expression is the planted answer: a
+    search finds it or an equivalent expression of at most its size."""
+    rng = SplitMix64(seed)
+    n_terms = n_vars + (1 if const_one else 0)
+    mask = M64 if word_bits == 64 else 0xFFFFFFFF
+    ins = np.zeros((n_samples, n_terms), dtype=np.uint64)
+    for i in range(n_samples):
+        for j in range(n_vars):
+            ins[i, j] = rng.next() & mask
+        if const_one:
+            ins[i, n_vars] = 1
+    outs = eval_postfix(postfix, ins if word_bits == 64 else ins.astype(np.uint32),
+                        word_bits).astype(np.uint64)
+    return Instance(n_terms, ins, outs, word_bits, postfix, const_one,
+                    {"size": len(postfix), "seed": seed, "planted": True})
 
 
 def iter_batch(n: int, seed0: int, sizes: Sequence[int], vars_: Sequence[int],

@@ -39,4 +39,8 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import os
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SIMBA_REFERENCE")
+    if not ref:
+        sys.exit("usage: python " + sys.argv[0] + " <reference checkout> (or SIMBA_REFERENCE)")
+    main(ref)

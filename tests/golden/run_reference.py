@@ -9,7 +9,9 @@ It also times unsatisfiable sweeps, which give the reference's
 candidate-evals/s.  Output: one JSON file (path = first argument) that is
 committed as ``tests/golden/ref_results_u32.json``; with ``--rtid`` after
 the path, the reference's RTid build alone (``oracle/_ref/simba_rtid``),
-committed as ``tests/golden/ref_results_rtid_u32.json``.
+committed as ``tests/golden/ref_results_rtid_u32.json``; with ``--u64``, the
+reference widened to 64-bit words (``oracle/_ref/simba_nocache_u64``) on
+``ref_instances_u64.json``, committed as ``tests/golden/ref_results_u64.json``.
 """
 import json
 import subprocess
@@ -26,6 +28,7 @@ from simba_b200.instances import make_instance  # noqa: E402
 
 SIMBA = ROOT / "oracle" / "_ref" / "simba_nocache"
 SIMBA_RTID = ROOT / "oracle" / "_ref" / "simba_rtid"
+SIMBA_U64 = ROOT / "oracle" / "_ref" / "simba_nocache_u64"
 VFB = ROOT / "oracle" / "_ref" / "vfb_full_cache"
 
 
@@ -62,6 +65,24 @@ def main_rtid(out_path: str) -> None:
     Path(out_path).write_text(json.dumps(res, indent=1))
 
 
+def main_u64(out_path: str) -> None:
+    """The widened 64-bit reference build on the 64-bit golden instances
+    (tests/golden/make_golden_u64.py); committed as
+    tests/golden/ref_results_u64.json."""
+    insts = json.loads((HERE / "ref_instances_u64.json").read_text())
+    res = {"simba_u64": []}
+    with tempfile.TemporaryDirectory() as td:
+        td = Path(td)
+        for idx, d in enumerate(insts):
+            p = td / f"inst_{idx}.json"
+            p.write_text(json.dumps(d))
+            r = run(SIMBA_U64, p, d["max_len"], 120)
+            r.update({"idx": idx, "max_len": d["max_len"], "set": d["set"]})
+            res["simba_u64"].append(r)
+            print(idx, d["set"], d["max_len"], r.get("expr"), r.get("seconds"), flush=True)
+    Path(out_path).write_text(json.dumps(res, indent=1))
+
+
 def main(out_path: str) -> None:
     insts = json.loads((HERE / "ref_instances_u32.json").read_text())
     res = {"simba": [], "vfb": [], "sweeps": []}
@@ -94,5 +115,7 @@ def main(out_path: str) -> None:
 if __name__ == "__main__":
     if len(sys.argv) > 2 and sys.argv[2] == "--rtid":
         main_rtid(sys.argv[1])
+    elif len(sys.argv) > 2 and sys.argv[2] == "--u64":
+        main_u64(sys.argv[1])
     else:
         main(sys.argv[1])

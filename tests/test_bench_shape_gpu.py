@@ -1,0 +1,109 @@
+"""Parity at the benchmarked shape: 3 variables + the constant 1 (4
+terminals), 64 uint64 samples, the default value tables (sizes <= 10), and
+answers planted at sizes 11, 12 and 13 (tests/golden/make_golden_u64.py).
+
+At these sizes every candidate is decided by the spine kernel: spines
+without & and | by the hash join, the others by nested compares.  A planted
+``v0 OP R`` with OP in + - * and no & / | in R lies on join spines; OP in
+& | puts an & / | level at the root, which is matched by nested compares.
+
+For each instance the GPU answer must
+  * be a match (oracle evaluation on every sample) of at most the planted size,
+  * carry the rank of its own postfix (rank_of is the inverse of unranking),
+  * be the minimum matching rank of its (size, operator) block: the oracle
+    scans every rank of the block below it and finds none,
+  * report the reference rule's candidate counts per size,
+  * equal the one-thread-per-rank engine's answer (the reference's
+    per-rank algorithm on the GPU, which sweeps every rank of every block),
+  * lie in the same size and block as the widened 64-bit reference
+    executable's answer (tests/golden/ref_results_u64.json), whose
+    expression the oracle also verifies.
+"""
+import json
+from pathlib import Path
+
+import pytest
+
+import simba_b200 as S
+from simba_b200.instances import Instance, infix_to_postfix
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+OPS = "~&|^#+-*"
+
+
+def bench_cases():
+    insts = json.loads((GOLD / "ref_instances_u64.json").read_text())
+    return [(i, d) for i, d in enumerate(insts) if d["set"] == "bench_shape"]
+
+
+def reference_answers():
+    f = GOLD / "ref_results_u64.json"
+    if not f.exists():
+        return {}
+    return {r["idx"]: r for r in json.loads(f.read_text())["simba_u64"]}
+
+
+@pytest.mark.parametrize("idx,d", bench_cases(), ids=lambda x: str(x) if isinstance(x, int) else "")
+def test_planted_answer_at_bench_shape(oracle, idx, d):
+    inst = Instance.from_json(d)
+    assert inst.num_variables == 4 and inst.num_examples == 64 and inst.word_bits == 64
+    size = d["gen_size"]
+    res = S.solve(inst, d["max_len"])
+    assert res.found and 2 <= res.size <= size
+    assert res.table_size == 10  # default tables: the spine kernel decides sizes 11-13
+    assert oracle.check(res.postfix, inst.inputs, inst.outputs, 64)
+    assert S.rank_of(res.postfix, 4) == res.rank
+    t = oracle.count_table(res.size, 4)
+    lo = int(sum(int(x) for x in t[res.size][: res.op]))
+    assert lo <= res.rank < lo + int(t[res.size][res.op])
+    # no rank of the block below the GPU's answer matches
+    ev, mr, nh = oracle.scan_range(inst.inputs, inst.outputs, res.size, lo, res.rank + 1, 64)
+    assert nh >= 1 and mr == res.rank
+    # reference-rule counts: whole sizes below, the answer's size up to its block
+    for s in range(2, res.size):
+        assert res.per_size[s] == int(t[s][8])
+    assert res.per_size[res.size] == int(sum(int(x) for x in t[res.size][: res.op + 1]))
+    # the per-rank engine sweeps the same blocks rank by rank
+    nv = S.solve(inst, d["max_len"], naive=True)
+    assert (nv.status, nv.size, nv.op, nv.rank, nv.postfix, nv.candidates) == \
+        (res.status, res.size, res.op, res.rank, res.postfix, res.candidates)
+    ref = reference_answers().get(idx)
+    if ref is not None:
+        p = infix_to_postfix(ref["expr"])
+        assert oracle.check(p, inst.inputs, inst.outputs, 64)
+        assert (len(p), OPS.index(p[-1])) == (res.size, res.op)
+
+
+def test_planted_answers_keep_their_size():
+    """The planted expressions were chosen without an equivalent of size
+    <= 10; most must be found at exactly the planted size, so that the
+    join and nested-compare paths at sizes 11-13 are the ones answering."""
+    at_size = 0
+    for _, d in bench_cases():
+        res = S.solve(Instance.from_json(d), d["max_len"])
+        at_size += res.size == d["gen_size"]
+    assert at_size >= 4
+
+
+def test_golden_u64_reference_instances(oracle):
+    """Random 64-bit instances: the GPU equals the oracle rank for rank, and
+    lies in the widened reference executable's size and block."""
+    insts = json.loads((GOLD / "ref_instances_u64.json").read_text())
+    refs = reference_answers()
+    for idx, d in enumerate(insts):
+        if d["set"] != "random":
+            continue
+        inst = Instance.from_json(d)
+        res = S.solve(inst, d["max_len"])
+        o = oracle.search(inst.inputs, inst.outputs, d["max_len"], 64)
+        assert (res.found, res.size, res.op, res.rank, res.postfix, res.candidates) == \
+            (o["found"], o["size"], o["op"], o["rank"], o["postfix"], o["candidates"])
+        ref = refs.get(idx)
+        if ref is None:
+            continue
+        if ref["expr"] == "Not found !":
+            assert not res.found
+            continue
+        p = infix_to_postfix(ref["expr"])
+        assert (len(p), OPS.index(p[-1])) == (res.size, res.op)

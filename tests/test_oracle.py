@@ -226,3 +226,38 @@ def test_oracle_rtid_matches_reference_rtid(oracle):
         assert o["found"] and len(p) == o["size"] and OPS.index(p[-1]) == o["op"]
         same += p == o["postfix"]
     assert same >= 100
+
+
+def test_oracle_matches_widened_reference_u64(oracle):
+    """The reference widened to 64-bit words (oracle/build_ref.sh,
+    simba_nocache_u64) on the 64-bit golden instances: its expression
+    verifies under the oracle's uint64 arithmetic and lies in the oracle's
+    size and operator block (random set, sizes 3-10); for the planted
+    bench-shape answers (sizes 11-13, too large for a CPU sweep) the
+    reference's expression verifies and has at most the planted size."""
+    import json
+    from pathlib import Path
+    g = Path(__file__).resolve().parent / "golden"
+    f = g / "ref_results_u64.json"
+    if not f.exists():
+        pytest.skip("widened reference results not generated")
+    insts = json.loads((g / "ref_instances_u64.json").read_text())
+    same = 0
+    for r in json.loads(f.read_text())["simba_u64"]:
+        d = insts[r["idx"]]
+        inst = Instance.from_json(d)
+        assert inst.word_bits == 64
+        if r["expr"] == "Not found !":
+            assert d["set"] == "random"
+            o = oracle.search(inst.inputs, inst.outputs, r["max_len"], 64)
+            assert not o["found"]
+            continue
+        p = infix_to_postfix(r["expr"])
+        assert oracle.check(p, inst.inputs, inst.outputs, 64)
+        if d["set"] == "bench_shape":
+            assert len(p) <= d["gen_size"]
+            continue
+        o = oracle.search(inst.inputs, inst.outputs, r["max_len"], 64)
+        assert o["found"] and (len(p), OPS.index(p[-1])) == (o["size"], o["op"])
+        same += p == o["postfix"]
+    assert same >= 30
