@@ -4,25 +4,26 @@
 Workload (one GPU): the larger plain-search configuration -- a target over 3
 variables + the constant 1 (4 terminals), 64 uniform uint64 samples
 (SplitMix64 seed 1) -- with the outputs replaced by random words so that no
-expression matches and every candidate of sizes 2..L is evaluated (L = 14 by
-default: 9.7e11 candidates per step).  A step is one sweep of those sizes:
+expression matches and every candidate of sizes 2..L is evaluated (L = 13 by
+default: 1.12e11 candidates per step).  A step is one sweep of those sizes:
 exactly the blocks the reference launches for `simba <instance> L+1`.
 
 value     candidates / second with samples and value tables resident in HBM
           (session API), timed with CUDA events on the launching stream.
 e2e       the same metric through simba_solve() from host buffers: H2D of the
           samples, table build, search, D2H of the result, every step.
-roofline  the search kernel's integer lane-operations (nested compares: the
-          masked compare and explicitly evaluated levels per candidate; hash
-          join: hash and filter test per bottom value and context block) over
-          the measured int32 issue peak of the device (simba_int_peak).
+roofline  the dominant launch kind of the search kernel (see roofline()).
 cpu_baseline  the OpenMP oracle (a port of the reference's per-rank
           unrank + evaluate) on a bounded sample of size-L ranks.
+Secondary objects (one GPU only, outside the timed region): the sizes 2..14
+sweep, the 4096-instance batch, and VFB on the same instance.
 
---impl reference runs the reference's own CUDA executable (rebuilt for
-sm_100a into oracle/_ref/) on the uint32 version of the same workload,
-sweeping sizes 2..13, and reports its candidate-evals/s from its own timer
-minus the CUDA context start-up it also times.
+--impl reference runs the reference's own CUDA executable, rebuilt for
+sm_100a from its sources with its words widened to uint64_t
+(oracle/build_ref.sh -> oracle/_ref/simba_nocache_u64), on the same
+instance file and the same sizes, and reports candidate-evals/s from its own
+timer minus the CUDA context start-up it also times.  It loads nothing of
+this repository's libraries.
 
 Multi-GPU: one process per GPU (torchrun); every rank sweeps its own
 independent instance (seed 1 + rank), no data-path collective: weak scaling.
@@ -43,8 +44,8 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-SWEEP_L = 14
-REF_L = 13
+SWEEP_L = 13   # sizes 2..13: the blocks of `simba <instance> 14`
+LARGE_L = 14
 N_VARS, N_SAMPLES, TARGET_SIZE = 3, 64, 15
 
 
@@ -57,14 +58,17 @@ def parse():
     ap.add_argument("--sweep", type=int, default=SWEEP_L)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--case", choices=["spine12", "batch10", "vfb10"],
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the secondary objects (larger sweep, batch, VFB)")
+    ap.add_argument("--case", choices=["spine12", "sweep13", "batch10", "vfb10"],
                     help="run one small profiling case instead of the benchmark (no JSON line)")
     return ap.parse_args()
 
 
 def run_case(name: str) -> None:
     """Small cases for ncu captures (see profiles/): a size-12 sweep of the
-    benchmark instance run twice; a 256-instance mixed batch to max size 11
+    benchmark instance run twice; the sizes 2..13 sweep run twice (the
+    launch list of one benchmark step); a 256-instance mixed batch to max size 11
     (its 9th spine launch is the size-10 round); VFB to maxLen 10 on the
     benchmark instance."""
     sys.path.insert(0, str(ROOT))
@@ -76,6 +80,11 @@ def run_case(name: str) -> None:
             for _ in range(2):
                 r = ss.sweep(12, 12)
         print("spine12", r.candidates, r.evaluated, r.kernel_ms)
+    elif name == "sweep13":
+        with S.Session(inst, verbose=True) as ss:
+            for _ in range(2):
+                r = ss.sweep(2, 13)
+        print("sweep13", r.candidates, r.evaluated, r.kernel_ms)
     elif name == "batch10":
         insts = list(iter_batch(256, 5 * 10 ** 6, sizes=range(7, 20), vars_=(2, 3, 4, 5),
                                 samples=(32, 64, 128), word_bits=64))
@@ -144,10 +153,27 @@ def make_workload(seed: int, bits: int):
                          unsat=True)
 
 
+def count_totals(max_size: int, k: int) -> list:
+    """Candidates per size of the reference's rank space (the column-8 totals
+    of numForm, simba/src/nocache.cu:117-160), in plain Python integers so
+    that the reference arm loads no library of this repository: size 1 has
+    k terminals, size 2 the two unary operators over them, and size s >= 3
+    two unary blocks of N(s-1), five commutative binary blocks over the
+    splits with left size <= (s-1)/2, and `-` over every split."""
+    n = [0] * (max_size + 1)
+    if max_size >= 1:
+        n[1] = k
+    if max_size >= 2:
+        n[2] = 2 * k
+    for s in range(3, max_size + 1):
+        comm = sum(n[j] * n[s - 1 - j] for j in range(1, (s - 1) // 2 + 1))
+        every = sum(n[j] * n[s - 1 - j] for j in range(1, s - 1))
+        n[s] = 2 * n[s - 1] + 5 * comm + every
+    return n
+
+
 def sweep_candidates(k: int, lo: int, hi: int) -> int:
-    from simba_b200 import count_table
-    t = count_table(hi, k)
-    return int(sum(int(t[s][8]) for s in range(lo, hi + 1)))
+    return sum(count_totals(hi, k)[lo:hi + 1])
 
 
 def cpu_baseline(inst, size: int) -> dict:
@@ -165,6 +191,87 @@ def cpu_baseline(inst, size: int) -> dict:
     return {"value": ev / dt, "unit": "candidate-evals/s", "cores": cores, "kind": "port",
             "sample": f"first {ev} ranks of size {size}, {N_SAMPLES} uint64 samples, "
                       f"{N_VARS} vars + const 1, unsatisfiable target ({dt:.1f} s)"}
+
+
+def pct(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    return xs[min(len(xs) - 1, int(q * len(xs)))]
+
+
+def secondary(a, S, sess, inst, device: int, stream) -> dict:
+    """Measurements beside the headline, on one GPU, outside its timed
+    region: the larger sizes 2..14 sweep (same instance, resident), the
+    4096-instance batch (target size 5-15, 1-4 variables + 1, samples
+    {16,32,64,128}, max size 18, autotuned work units, 60 s budget; times on
+    the device clock) and VFB on the same instance (satisfiable target, and
+    the unsatisfiable sweep to maxLen 11: cache bytes and algorithmic HBM
+    bytes per second)."""
+    import torch
+    from simba_b200 import autotune
+    from simba_b200.instances import iter_batch, make_instance
+    out = {}
+    L = LARGE_L
+    cand = sweep_candidates(inst.num_variables, 2, L)
+    sess.sweep(2, L)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    n = 3
+    torch.cuda.synchronize()
+    e0.record(stream)  # the session launches on this stream
+    ks = 0.0
+    for _ in range(n):
+        r = sess.sweep(2, L)
+        assert r.status == S.NOT_FOUND and r.candidates == cand, r
+        ks += r.kernel_ms
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out["sweep_2_14"] = {"value": cand * n / (ms / 1e3), "unit": "candidate-evals/s",
+                         "ms_per_step": ms / n, "candidates_per_step": cand,
+                         "kernel_ms_per_step": ks / n, "steps": n}
+
+    insts = list(iter_batch(4096, 0, sizes=range(5, 16), vars_=(1, 2, 3, 4),
+                            samples=(16, 32, 64, 128), word_bits=64))
+    tuned = autotune.tune_batch(insts, device=device)
+    for i in insts:
+        i.unit_log2 = tuned[(i.num_variables, i.num_examples, i.word_bits)]
+    t0 = time.perf_counter()
+    res, st = S.solve_batch(insts, 18, budget=60, device=device)
+    wall = time.perf_counter() - t0
+    solved = [r.seconds for r in res if r.status == S.OK]
+    every = [r.seconds if r.status == S.OK else float("inf") for r in res]
+    out["batch_4096"] = {
+        "workload": "4096 instances: target size 5-15, 1-4 vars + const 1, samples "
+                    "{16,32,64,128}, uint64, max size 18, 60 s budget, seeds 0-4095",
+        "solved_frac": len(solved) / len(res), "p50_s": pct(every, 0.5), "p95_s": pct(every, 0.95),
+        "p50_solved_s": pct(solved, 0.5), "p95_solved_s": pct(solved, 0.95),
+        "candidate_evals_per_kernel_s": st["evaluated"] / max(st["kernel_ms"] / 1e3, 1e-9),
+        "rounds": st["rounds"], "launches": st["launches"], "wall_s": wall,
+        "units": {f"k{k[0]}_S{k[1]}": v for k, v in sorted(tuned.items())}}
+
+    sat = make_instance(TARGET_SIZE, N_VARS, N_SAMPLES, 1, word_bits=64)
+    v1 = S.vfb_solve(sat, 20, budget=60, device=device)
+    S.vfb_solve(inst, 9, device=device)  # warm-up
+    v2 = S.vfb_solve(inst, 11, budget=120, device=device)
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        pass
+    hbm = peaks.get("hbm_gbs")
+    gbs = v2.bytes_moved / max(v2.device_ms / 1e3, 1e-9) / 1e9
+    out["vfb"] = {
+        "satisfiable": {"status": v1.status, "size": v1.size, "expr": v1.expr,
+                        "device_ms": v1.device_ms, "candidates": v1.candidates,
+                        "rows": v1.rows_total},
+        "sweep_maxlen_11": {"status": v2.status, "candidates": v2.candidates, "rows": v2.rows_total,
+                            "cache_bytes": v2.cache_bytes, "device_ms": v2.device_ms,
+                            "candidate_evals_per_s": v2.candidates / max(v2.device_ms / 1e3, 1e-9),
+                            "algorithmic_gbs": gbs, "hbm_gbs_measured": hbm,
+                            "frac": gbs / hbm if hbm else None}}
+    return out
 
 
 def run_ours(a, rank: int, world: int, local_rank: int) -> None:
@@ -242,15 +349,8 @@ def run_ours(a, rank: int, world: int, local_rank: int) -> None:
         alu_peak = S.alu_peak(local_rank)
         kernel_s = kernel_ms / 1e3
         achieved = alg_ops / kernel_s if kernel_s > 0 else 0.0
+        # DRAM traffic needs an ncu capture (profiles/); a live run cannot count it
         traffic = None
-        prof = ROOT / "profiles" / "spine_kernel_size12_u64_full.md"
-        if prof.exists():
-            import re
-            m = re.search(r"\|\s*dram_bytes_per_candidate\s*\|\s*([0-9.eE+-]+)", prof.read_text())
-            if m:
-                # DRAM bytes per candidate from the ncu capture, times the
-                # candidates of one average spine-kernel launch
-                traffic = float(m.group(1)) * evaluated / max(1, a.steps * (L - 1))
         out = {
             "metric": "candidate-evals/s", "value": value, "unit": "candidate-evals/s",
             "n_gpus": world, "steps": a.steps, "warmup": max(a.warmup, 3),
@@ -259,9 +359,11 @@ def run_ours(a, rank: int, world: int, local_rank: int) -> None:
             "config": {"workload": f"plain-search sweep of sizes 2..{L}: {N_VARS} vars + const 1 "
                                    f"(4 terminals), {N_SAMPLES} uint64 samples, SplitMix64 seed 1+rank, "
                                    "unsatisfiable target (the size-15 config with its outputs "
-                                   "randomised so every block is searched)",
+                                   "randomised so every block is searched); the reference arm "
+                                   "runs the same file and sizes",
                        "candidates_per_step": cand_step, "engine": "tabled spine kernel",
-                       "l2": "inputs larger than L2 (value tables of 4 samples up to 5.8 GB)",
+                       "same_config": True,
+                       "l2": "inputs larger than L2 (sample-0 value tables of sizes <= 10: 1.46 GB)",
                        "parallelism": f"independent instances x{world}"},
             "e2e": e2e,
             "roofline": {"bound": "int-alu", "achieved": achieved / 1e12, "peak": peak / 1e12,
@@ -275,6 +377,8 @@ def run_ours(a, rank: int, world: int, local_rank: int) -> None:
             "gpu_launches": launches,
             "clocks": clk,
         }
+        if world == 1 and not a.no_secondary:
+            out.update(secondary(a, S, sess, inst, local_rank, stream))
         if not a.no_cpu:
             try:
                 out["cpu_baseline"] = cpu_baseline(inst, L)
@@ -287,19 +391,25 @@ def run_ours(a, rank: int, world: int, local_rank: int) -> None:
 
 
 def run_reference(a, rank: int) -> None:
-    """The reference's own CUDA build on the uint32 version of the workload."""
+    """The reference's own CUDA build (words widened to uint64_t) on the same
+    instance and sizes as this repository's arm.  Nothing of this
+    repository's native code is loaded: the instance generator is numpy, the
+    candidate count is plain Python and the timed work is the reference
+    executable."""
     if rank != 0:
         return
-    exe = ROOT / "oracle" / "_ref" / "simba_nocache"  # built by __graft_entry__.build()
-    inst = make_workload(1, 32)
-    L = REF_L
+    exe = ROOT / "oracle" / "_ref" / "simba_nocache_u64"  # built by __graft_entry__.build()
+    inst = make_workload(1, 64)
+    L = a.sweep
     cand = sweep_candidates(inst.num_variables, 2, L)
-    cfg = {"workload": f"plain-search sweep of sizes 2..{L}: {N_VARS} vars + const 1, {N_SAMPLES} "
-                       "samples, unsatisfiable target; uint32 (the reference has no uint64 path)",
-           "candidates_per_step": cand}
+    cfg = {"workload": f"plain-search sweep of sizes 2..{L}: {N_VARS} vars + const 1 (4 terminals), "
+                       f"{N_SAMPLES} uint64 samples, SplitMix64 seed 1, unsatisfiable target",
+           "candidates_per_step": cand, "same_config": True,
+           "engine": "reference simba/src/nocache.cu with uint32_t widened to uint64_t "
+                     "(oracle/build_ref.sh), one thread per rank"}
     if not exe.exists():
         print(json.dumps({"impl": "reference", "unavailable": "reference executable not built "
-                          "(oracle/_ref/simba_nocache missing)"}))
+                          "(oracle/_ref/simba_nocache_u64 missing)"}))
         return
     with tempfile.TemporaryDirectory() as td:
         p = Path(td) / "sweep.json"
@@ -307,25 +417,29 @@ def run_reference(a, rank: int) -> None:
 
         def once(max_len: int) -> float:
             r = subprocess.run([str(exe), str(p), str(max_len)], capture_output=True, text=True,
-                               timeout=600)
+                               timeout=900)
             line = r.stdout.strip().splitlines()[-1]
-            return float(line.rsplit(",", 1)[1])
+            path, expr, secs = line.rsplit(",", 2)
+            if max_len > 2 and expr != "Not found !":
+                raise RuntimeError(f"reference found {expr} on an unsatisfiable target")
+            return float(secs)
 
         init = statistics.median([once(2) for _ in range(max(a.warmup, 3))])
-        for _ in range(1):
-            once(L + 1)
+        once(L + 1)  # warm-up sweep
         steps = [once(L + 1) for _ in range(a.steps)]
     search = [max(t - init, 1e-9) for t in steps]
     value = cand / statistics.mean(search)
     out = {"impl": "reference", "metric": "candidate-evals/s", "value": value,
            "unit": "candidate-evals/s", "n_gpus": 1, "steps": a.steps, "warmup": max(a.warmup, 3),
            "ms_per_step": statistics.mean(search) * 1e3, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+           "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
            "config": cfg,
-           "cpu_baseline": {"kind": "reference", "value": value, "unit": "candidate-evals/s",
-                            "cores": 1, "sample": f"reference CUDA executable rebuilt for sm_100a "
-                            f"(GPU; 1 host thread), sizes 2..{L}; its own timer minus the "
-                            f"{init:.3f} s CUDA start-up measured with maxLen 2"},
+           "reference_build": {"kind": "reference", "device": "gpu", "cores": 1,
+                               "sample": f"the whole sweep of sizes 2..{L} per step "
+                                         f"(`simba_nocache_u64 <instance> {L + 1}`), its own "
+                                         f"printed seconds minus the {init:.3f} s CUDA start-up "
+                                         "it also times (measured with maxLen 2); the reference "
+                                         "has no CPU implementation"},
            "e2e": {"value": value, "unit": "candidate-evals/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0},
            "reference_seconds_per_step_incl_context": statistics.mean(steps)}

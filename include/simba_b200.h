@@ -17,7 +17,7 @@
 extern "C" {
 #endif
 
-#define SIMBA_ABI_VERSION 1
+#define SIMBA_ABI_VERSION 2
 
 /* Status codes (return value of the solve calls and result.status). */
 #define SIMBA_OK 0           /* an expression was found                      */
@@ -81,7 +81,18 @@ typedef struct {
                             match with the smallest t is returned; c is the
                             smallest integer >= 2246822507 coprime to N, so
                             every rank is visited exactly once            */
-  int32_t reserved;
+  int32_t grammar;       /* simba_solve and vfb_solve only.  0: the reference's
+                            operators ~ & | ^ neg + - *.  1: the extended set
+                            the reference declares but leaves switched off
+                            (vfb/src/full-cache.cu:166-179,460-472):
+                            ~ & | ^ << >> neg + - * / % in that order, postfix
+                            characters < > / %, result op codes 9..12 for
+                            << >> / %; shifts by >= the word width give 0;
+                            VFB takes the dividend vector when any divisor
+                            element is 0 (full-cache.cu:230-256), the plain
+                            search the dividend per sample (x/0 = x%0 = x);
+                            at most 10 terminals.  The plain search runs one
+                            thread per rank in this grammar.               */
 } simba_options;
 
 typedef struct {
@@ -102,6 +113,17 @@ typedef struct {
   double kernel_ms;      /* GPU time of the search kernel launches alone         */
   uint64_t alg_ops;      /* integer lane-operations the algorithm needs for the
                             candidates evaluated (see simba_int_peak)            */
+  /* The spine kernel runs up to two launches per size: the hash-join units
+   * (spines without & and |) and the nested-compare units.  Their GPU time
+   * and candidates, summed over the sizes searched: */
+  double join_ms;
+  double nested_ms;
+  uint64_t join_candidates;
+  uint64_t nested_candidates;
+  double join_bytes_streamed; /* bottom-table bytes the join units read: each
+                            table once per block of contexts                    */
+  double join_table_bytes;    /* the bottom tables the join launches read, each
+                            counted once per size: the algorithmic minimum     */
 } simba_result;
 
 /* Plain cache-free unranking search of one instance: replaces NoCache::solve
@@ -140,16 +162,24 @@ int vfb_solve(const simba_instance *inst, int max_len, const simba_options *opt,
               vfb_result *result);
 
 /* simba_solve without any device allocation, for callers that cannot call
- * cudaMalloc while they run (a plugin inside a host application that owns
- * the GPU memory budget, or code running while another stream is being
- * captured into a CUDA graph).  No counterpart in the reference.  All
- * scratch lives in one 64 MiB __device__ array that every GPU loading the
- * library holds until exit; sizes whose value tables or spine list do not
- * fit it are rejected with SIMBA_E_ARG.  The first call on a device looks up
- * that array's address, so make it before any stream capture starts.  Calls
- * share the array: calls that overlap on the GPU race and must be
- * serialised.  Runs on opt->stream (0 = default stream); creates no stream
- * or event and reports only host-clock seconds. */
+ * cudaMalloc while they run: a plugin inside a host application that owns
+ * the GPU memory budget (its own pool allocator must not be bypassed), or
+ * work issued while another stream of the process is being captured into a
+ * CUDA graph, where an allocation would invalidate that capture.  No
+ * counterpart in the reference.  All scratch lives in one 64 MiB __device__
+ * array that every GPU loading the library holds until exit; sizes whose
+ * value tables or spine list do not fit it are rejected with SIMBA_E_ARG.
+ * The first call on a device looks up that array's address, so make it
+ * before any stream capture starts; the address is cached per device
+ * ordinal and is not valid after cudaDeviceReset.  Calls share the array:
+ * calls that overlap on the GPU race and must be serialised.  Runs on
+ * opt->stream; while another stream is being captured, pass a non-blocking
+ * stream (cudaStreamNonBlocking or the per-thread default stream), since
+ * work on the legacy default stream (stream 0) synchronises with blocking
+ * streams, and capture that other stream in relaxed or thread-local mode.
+ * Plain spine search only: opt->engine must be 0 and opt->class_prior NULL
+ * (SIMBA_E_ARG otherwise); opt->table_bytes and opt->unit_log2 are ignored.
+ * Creates no stream or event and reports only host-clock seconds. */
 int simba_solve_noalloc(const simba_instance *inst, int max_size, const simba_options *opt,
                         simba_result *result);
 
@@ -236,7 +266,8 @@ int simba_unrank(uint64_t rank, int size, int n_terms, char *postfix);
 /* Postfix -> rank (inverse of simba_unrank). */
 int simba_rank_of(const char *postfix, int n_terms, uint64_t *rank);
 /* Postfix -> infix; style 0 = SIMBA (nocache.cu:162-195), 1 = VFB
- * (vfb/src/full-cache.cu:483-509).  Returns the length or a negative code. */
+ * (vfb/src/full-cache.cu:483-509); add 2 to read '<' '>' '/' '%' as the
+ * extended grammar's << >> / %.  Returns the length or a negative code. */
 int simba_format(const char *postfix, int style, char *out, int cap);
 
 /* Instance file reader: the reference JSON schema (simba/src/instance.cpp:7-27,

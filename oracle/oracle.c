@@ -645,3 +645,358 @@ done:
   free(v);
   return rc < 0 ? rc : res->found;
 }
+
+/* ---------------------------------------------------------------------------
+ * Extended grammar: the operator set of the reference's Op enum with the
+ * shifts, division and modulo that its builds leave switched off
+ * (vfb/src/full-cache.cu:166-179 declares Not And Or Xor LShift RShift Neg
+ * Plus Minus Mul Div Mod; :460-472 comments LShift, RShift, Div and Mod out
+ * of the enumeration; simba/src/mba.cuh:71-131 evaluates '<' '>' '/' '%' in
+ * evaluateRPN, which nothing calls).  Operator order, as declared:
+ *   ~ & | ^ << >> neg + - * / %     (postfix chars ~ & | ^ < > # + - * / %)
+ * Rank space: the SIMBA count recurrence with the four new binary operators
+ * counted like '-' (every left size; none is commutative).
+ * Semantics on w-bit words: x << y and x >> y (logical) are 0 when y >= w,
+ * as the GPU's clamped shifts give for the reference's `L[i] << R[i]`
+ * (full-cache.cu:215-220).  Division and modulo follow VFB's zero-divisor
+ * rule (full-cache.cu:230-256): in VFB, where whole vectors are composed, a
+ * divisor vector with any zero element makes the result the dividend vector;
+ * the SIMBA rank-space search evaluates one sample at a time and applies the
+ * same fallback per sample (x / 0 = x % 0 = x).
+ * Operator codes in results: the base codes 0..7, 9 '<<', 10 '>>', 11 '/',
+ * 12 '%' (8 stays "a variable").
+ * ------------------------------------------------------------------------- */
+
+#define EXT_OPS 12
+#define EXT_COLS 13
+static const char EXT_CHARS[EXT_OPS] = {'~', '&', '|', '^', '<', '>', '#', '+', '-', '*', '/', '%'};
+static const int EXT_CODE[EXT_OPS] = {0, 1, 2, 3, 9, 10, 4, 5, 6, 7, 11, 12};
+
+static int ext_unary(int e) { return e == 0 || e == 6; }
+static int ext_comm(int e) { return e == 1 || e == 2 || e == 3 || e == 7 || e == 9; }
+
+static char code_char(int code) {
+  switch (code) {
+    case 9: return '<';
+    case 10: return '>';
+    case 11: return '/';
+    case 12: return '%';
+  }
+  return OP_CHARS[code];
+}
+
+int orc_ext_count_table(int max_size, int n_terms, uint64_t *t) {
+  int overflow = 0;
+  memset(t, 0, sizeof(uint64_t) * EXT_COLS * (size_t)(max_size + 1));
+  if (max_size >= 1) t[1 * EXT_COLS + EXT_OPS] = (uint64_t)n_terms;
+  if (max_size >= 2) {
+    t[2 * EXT_COLS + 0] = (uint64_t)n_terms;
+    t[2 * EXT_COLS + 6] = (uint64_t)n_terms;
+    t[2 * EXT_COLS + EXT_OPS] = 2 * (uint64_t)n_terms;
+  }
+  for (int i = 3; i <= max_size; ++i) {
+    unsigned __int128 u = t[(i - 1) * EXT_COLS + EXT_OPS], c = 0, n = 0, tot = 0;
+    for (int j = 1; j <= (i - 1) / 2; ++j)
+      c += (unsigned __int128)t[j * EXT_COLS + EXT_OPS] * t[(i - j - 1) * EXT_COLS + EXT_OPS];
+    for (int j = 1; j <= i - 2; ++j)
+      n += (unsigned __int128)t[j * EXT_COLS + EXT_OPS] * t[(i - j - 1) * EXT_COLS + EXT_OPS];
+    for (int e = 0; e < EXT_OPS; ++e) {
+      const unsigned __int128 v = ext_unary(e) ? u : (ext_comm(e) ? c : n);
+      if (v >> 64) overflow = 1;
+      t[i * EXT_COLS + e] = (uint64_t)v;
+      tot += v;
+    }
+    if (tot >> 64) overflow = 1;
+    t[i * EXT_COLS + EXT_OPS] = (uint64_t)tot;
+  }
+  return overflow ? -1 : 0;
+}
+
+static void ext_unrank_rec(uint64_t n, int size, const uint64_t *t, char *out) {
+  if (size == 1) {
+    out[0] = (char)('0' + (int)n);
+    return;
+  }
+  uint64_t part = 0;
+  int e = 0;
+  while (n >= part + t[size * EXT_COLS + e]) part += t[size * EXT_COLS + e++];
+  n -= part;
+  const int sub = size - 1;
+  out[sub] = EXT_CHARS[e];
+  if (ext_unary(e)) {
+    ext_unrank_rec(n, sub, t, out);
+    return;
+  }
+  uint64_t fpart = 0;
+  int f = 1;
+  while (n >= fpart + t[f * EXT_COLS + EXT_OPS] * t[(sub - f) * EXT_COLS + EXT_OPS]) {
+    fpart += t[f * EXT_COLS + EXT_OPS] * t[(sub - f) * EXT_COLS + EXT_OPS];
+    f++;
+  }
+  n -= fpart;
+  const uint64_t r = t[(sub - f) * EXT_COLS + EXT_OPS];
+  ext_unrank_rec(n / r, f, t, out);
+  ext_unrank_rec(n % r, sub - f, t, out + f);
+}
+
+void orc_ext_unrank(uint64_t rank, int size, const uint64_t *t, char *postfix) {
+  ext_unrank_rec(rank, size, t, postfix);
+}
+
+/* One operator on one sample (the per-sample form of the rules above). */
+static inline uint64_t ext_apply(char c, uint64_t l, uint64_t r, int bits) {
+  const uint64_t m = wmask(bits);
+  switch (c) {
+    case '<': return r >= (uint64_t)bits ? 0 : (l << r) & m;
+    case '>': return r >= (uint64_t)bits ? 0 : l >> r;
+    case '/': return r == 0 ? l : l / r;
+    case '%': return r == 0 ? l : l % r;
+  }
+  return apply_op(c, l, r, m);
+}
+
+uint64_t orc_ext_eval1(const char *p, int len, int bits, const uint64_t *row) {
+  uint64_t st[ORC_MAX_SIZE + 8];
+  int sp = -1;
+  const uint64_t m = wmask(bits);
+  for (int j = 0; j < len; ++j) {
+    const char c = p[j];
+    if (c == '~' || c == '#') {
+      st[sp] = ext_apply(c, 0, st[sp], bits);
+    } else if (c >= '0' && c <= '9') {  /* at most 10 terminals: '<' and '>' follow '9' */
+      st[++sp] = row[c - '0'] & m;
+    } else {
+      const uint64_t r = st[sp--];
+      st[sp] = ext_apply(c, st[sp], r, bits);
+    }
+  }
+  return st[0];
+}
+
+int orc_ext_check(const char *p, int len, int bits, int k, int S, const uint64_t *in,
+                  const uint64_t *out) {
+  const uint64_t m = wmask(bits);
+  for (int i = 0; i < S; ++i)
+    if (orc_ext_eval1(p, len, bits, in + (size_t)i * k) != (out[i] & m)) return 0;
+  return 1;
+}
+
+/* The plain search in the extended grammar: sizes 2 .. max_size-1 (1 and
+ * max_size too with include_edges), the twelve operator blocks of a size in
+ * order, stop after the first block with a match, minimum matching rank of
+ * that block (the rules of orc_search).  res->op is the operator's code. */
+int orc_ext_search(int bits, int k, int S, const uint64_t *in, const uint64_t *out, int max_size,
+                   int include_edges, int nth, orc_result *res) {
+  memset(res, 0, sizeof(*res));
+  if (max_size > ORC_MAX_SIZE || k > 10 || k < 1 || S < 1) return -2;
+  uint64_t t[(ORC_MAX_SIZE + 1) * EXT_COLS];
+  if (orc_ext_count_table(max_size, k, t) != 0) return -3;
+  if (nth <= 0) nth = orc_max_threads();
+  const uint64_t m = wmask(bits);
+  if (include_edges) {
+    for (int v = 0; v < k; ++v) {
+      res->candidates++;
+      res->per_size[1]++;
+      int ok = 1;
+      for (int i = 0; i < S && ok; ++i) ok = (in[(size_t)i * k + v] & m) == (out[i] & m);
+      if (ok) {
+        res->found = 1;
+        res->size = 1;
+        res->op = 8;
+        res->rank = (uint64_t)v;
+        res->postfix[0] = (char)('0' + v);
+        return 1;
+      }
+    }
+  }
+  const int last = include_edges ? max_size : max_size - 1;
+  for (int s = 2; s <= last; ++s) {
+    uint64_t off = 0;
+    for (int e = 0; e < EXT_OPS; ++e) {
+      const uint64_t N = t[s * EXT_COLS + e];
+      res->candidates += N;
+      res->per_size[s] += N;
+      uint64_t best = ~0ULL;
+      if (N) {
+        const int64_t nchunks = (int64_t)((N + ORC_CHUNK - 1) / ORC_CHUNK);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nth)
+#endif
+        for (int64_t c = 0; c < nchunks; ++c) {
+          const uint64_t a = off + (uint64_t)c * ORC_CHUNK;
+          const uint64_t b = a + ORC_CHUNK < off + N ? a + ORC_CHUNK : off + N;
+          if (a > __atomic_load_n(&best, __ATOMIC_RELAXED)) continue;
+          char p[ORC_MAX_SIZE + 1];
+          for (uint64_t r = a; r < b; ++r) {
+            orc_ext_unrank(r, s, t, p);
+            if (orc_ext_check(p, s, bits, k, S, in, out)) {
+              atomic_min_u64(&best, r);
+              break;
+            }
+          }
+        }
+      }
+      if (best != ~0ULL) {
+        res->found = 1;
+        res->size = s;
+        res->op = EXT_CODE[e];
+        res->rank = best;
+        orc_ext_unrank(best, s, t, res->postfix);
+        res->postfix[s] = 0;
+        return 1;
+      }
+      off += N;
+    }
+  }
+  return 0;
+}
+
+/* Whole-vector composition in the extended grammar (full-cache.cu:182-262):
+ * '/' and '%' copy the dividend vector when any divisor element is zero. */
+static void ext_compose(char c, const uint64_t *a, const uint64_t *b, uint64_t *v, int S, int bits) {
+  if (c == '/' || c == '%') {
+    int zero = 0;
+    for (int i = 0; i < S && !zero; ++i) zero = b[i] == 0;
+    if (zero) {
+      memcpy(v, a, sizeof(uint64_t) * S);
+      return;
+    }
+  }
+  for (int i = 0; i < S; ++i) v[i] = ext_apply(c, a[i], b[i], bits);
+}
+
+static int ext_row_postfix(const rowstore *rs, int64_t row, char *out, int pos, int maxlen) {
+  if (pos >= maxlen - 1) return -1;
+  const int op = rs->op[row];
+  if (op < 0) {
+    out[pos] = (char)('0' + (int)rs->l[row]);
+    return pos + 1;
+  }
+  pos = ext_row_postfix(rs, rs->l[row], out, pos, maxlen);
+  if (pos < 0) return -1;
+  if (op != ORC_NOT && op != ORC_NEG) {
+    pos = ext_row_postfix(rs, rs->r[row], out, pos, maxlen);
+    if (pos < 0) return -1;
+  }
+  if (pos >= maxlen - 1) return -1;
+  out[pos] = code_char(op);
+  return pos + 1;
+}
+
+/* VFB in the extended grammar: the driver of orc_vfb with the twelve
+ * operators in declaration order (the reference's generateMBAs, full-cache.cu:
+ * 568-663, with LShift, RShift, Div and Mod enabled; every non-commutative
+ * operator -- '-', '<<', '>>', '/', '%' -- also composes the swapped pair,
+ * :573-575), exact dedup (the documented intent; no as-written mode). */
+int orc_ext_vfb(int bits, int k, int S, const uint64_t *in, const uint64_t *out, int max_len,
+                int64_t cap_rows, orc_vfb_result *res) {
+  memset(res, 0, sizeof(*res));
+  if (max_len < 1 || max_len > 100 || S < 1 || k < 1 || k > 10) return -2;
+  const uint64_t m = wmask(bits);
+  vfb_state st;
+  memset(&st, 0, sizeof(st));
+  st.S = S;
+  st.cap_rows = cap_rows > 0 ? cap_rows : ((int64_t)1 << 40);
+  st.found_row = -1;
+  st.rows.S = S;
+  uint64_t *tgt = (uint64_t *)malloc(sizeof(uint64_t) * S);
+  uint64_t *v = (uint64_t *)malloc(sizeof(uint64_t) * S);
+  if (!tgt || !v || vs_init(&st.seen, S)) return -1;
+  for (int i = 0; i < S; ++i) tgt[i] = out[i] & m;
+  st.target = tgt;
+  int rc = 0;
+  int64_t start[102];
+  memset(start, 0, sizeof(start));
+  for (int j = 0; j < k; ++j) {
+    for (int i = 0; i < S; ++i) v[i] = in[(size_t)i * k + j] & m;
+    res->candidates++;
+    rs_push(&st.rows, v, -1, j, -1);
+    if (!memcmp(v, tgt, sizeof(uint64_t) * S)) {
+      res->found = 1;
+      res->size = 1;
+      res->op = 8;
+      res->postfix[0] = (char)('0' + j);
+      goto done;
+    }
+  }
+  for (int j = 0; j < k; ++j)
+    if (vs_insert(&st.seen, st.rows.vec + (size_t)j * S) < 0) {
+      rc = -1;
+      goto done;
+    }
+  res->rows_per_size[1] = k;
+  start[2] = st.rows.n;
+  for (int L = 2; L <= max_len; ++L) {
+    for (int e = 0; e < EXT_OPS && st.found_row < 0 && !st.full; ++e) {
+      const char c = EXT_CHARS[e];
+      const int code = EXT_CODE[e];
+      if (ext_unary(e)) {
+        for (int64_t x = start[L - 1]; x < start[L]; ++x) {
+          const uint64_t *a = st.rows.vec + x * S;
+          for (int i = 0; i < S; ++i) v[i] = ext_apply(c, 0, a[i], bits);
+          res->candidates++;
+          if (vfb_offer(&st, v, code, x, 0)) {
+            rc = -1;
+            goto done;
+          }
+        }
+        continue;
+      }
+      const int swap = !ext_comm(e);
+      for (int i = 1; 2 * i <= L - 1; ++i) {
+        const int j = L - 1 - i;
+        for (int64_t x = start[i]; x < start[i + 1]; ++x) {
+          for (int64_t y = start[j]; y < start[j + 1]; ++y) {
+            /* rows may move when the store grows: index them afresh */
+            ext_compose(c, st.rows.vec + x * S, st.rows.vec + y * S, v, S, bits);
+            res->candidates++;
+            if (vfb_offer(&st, v, code, x, y)) {
+              rc = -1;
+              goto done;
+            }
+            if (swap) {
+              ext_compose(c, st.rows.vec + y * S, st.rows.vec + x * S, v, S, bits);
+              res->candidates++;
+              if (vfb_offer(&st, v, code, y, x)) {
+                rc = -1;
+                goto done;
+              }
+            }
+          }
+        }
+      }
+      if (st.found_row >= 0) {
+        res->found = 1;
+        res->size = L;
+        res->op = code;
+        if (ext_row_postfix(&st.rows, st.found_row, res->postfix, 0, 256) < 0)
+          res->postfix[0] = 0;
+        break;
+      }
+    }
+    if (st.found_row >= 0 && !res->found) { /* found by a unary block */
+      res->found = 1;
+      res->size = L;
+      res->op = st.rows.op[st.found_row];
+      if (ext_row_postfix(&st.rows, st.found_row, res->postfix, 0, 256) < 0)
+        res->postfix[0] = 0;
+    }
+    start[L + 1] = st.rows.n;
+    res->rows_per_size[L] = st.rows.n - start[L];
+    if (st.found_row >= 0) break;
+    if (st.full) {
+      res->cache_full = 1;
+      break;
+    }
+  }
+done:
+  res->rows_total = st.rows.n;
+  vs_free(&st.seen);
+  free(st.rows.vec);
+  free(st.rows.op);
+  free(st.rows.l);
+  free(st.rows.r);
+  free(tgt);
+  free(v);
+  return rc < 0 ? rc : res->found;
+}

@@ -66,6 +66,20 @@ int orc_vfb(int word_bits, int n_terms, int n_samples, const uint64_t *inputs,
             const uint64_t *outputs, int max_len, int64_t cap_rows, int ref_inverted,
             orc_vfb_result *res);
 uint64_t orc_vfb_fingerprint32(const uint32_t *cs, int n);
+
+/* Extended grammar (~ & | ^ << >> neg + - * / %; see oracle.c): count table
+ * of (max_size + 1) rows x 13 columns (column 12 = total), unranking,
+ * per-sample evaluation, the plain search and VFB.  At most 10 terminals. */
+int orc_ext_count_table(int max_size, int n_terms, uint64_t *table);
+void orc_ext_unrank(uint64_t rank, int size, const uint64_t *table, char *postfix);
+uint64_t orc_ext_eval1(const char *postfix, int len, int word_bits, const uint64_t *row);
+int orc_ext_check(const char *postfix, int len, int word_bits, int n_terms, int n_samples,
+                  const uint64_t *inputs, const uint64_t *outputs);
+int orc_ext_search(int word_bits, int n_terms, int n_samples, const uint64_t *inputs,
+                   const uint64_t *outputs, int max_size, int include_edges, int n_threads,
+                   orc_result *res);
+int orc_ext_vfb(int word_bits, int n_terms, int n_samples, const uint64_t *inputs,
+                const uint64_t *outputs, int max_len, int64_t cap_rows, orc_vfb_result *res);
 int orc_max_threads(void);
 
 #ifdef __cplusplus

@@ -65,6 +65,15 @@ def lib():
         L.orc_vfb_fingerprint32.argtypes = [C.POINTER(C.c_uint32), C.c_int]
         L.orc_vfb_fingerprint32.restype = C.c_uint64
         L.orc_max_threads.restype = C.c_int
+        L.orc_ext_count_table.argtypes = [C.c_int, C.c_int, u64p]
+        L.orc_ext_unrank.argtypes = [C.c_uint64, C.c_int, u64p, C.c_char_p]
+        L.orc_ext_eval1.argtypes = [C.c_char_p, C.c_int, C.c_int, u64p]
+        L.orc_ext_eval1.restype = C.c_uint64
+        L.orc_ext_check.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, u64p, u64p]
+        L.orc_ext_search.argtypes = [C.c_int, C.c_int, C.c_int, u64p, u64p, C.c_int, C.c_int,
+                                     C.c_int, C.POINTER(OrcResult)]
+        L.orc_ext_vfb.argtypes = [C.c_int, C.c_int, C.c_int, u64p, u64p, C.c_int, C.c_int64,
+                                  C.POINTER(OrcVfbResult)]
         _lib = L
     return _lib
 
@@ -177,3 +186,63 @@ def fingerprint32(vec) -> int:
 
 def max_threads() -> int:
     return int(lib().orc_max_threads())
+
+
+# Extended grammar (~ & | ^ << >> neg + - * / %), see oracle.c.
+EXT_CHARS = "~&|^<>#+-*/%"
+
+
+def ext_count_table(max_size: int, n_terms: int) -> np.ndarray:
+    t = np.zeros((max_size + 1) * 13, dtype=np.uint64)
+    if lib().orc_ext_count_table(max_size, n_terms, _p(t)) != 0:
+        raise OverflowError("count table exceeds 64 bits")
+    return t.reshape(max_size + 1, 13)
+
+
+def ext_unrank(rank: int, size: int, table: np.ndarray) -> str:
+    buf = C.create_string_buffer(MAX_SIZE + 1)
+    t = _u64(table).reshape(-1)
+    lib().orc_ext_unrank(rank, size, _p(t), buf)
+    return buf.raw[:size].decode()
+
+
+def ext_eval1(postfix: str, row, word_bits: int = 64) -> int:
+    r = _u64(row)
+    return int(lib().orc_ext_eval1(postfix.encode(), len(postfix), word_bits, _p(r)))
+
+
+def ext_check(postfix: str, inputs, outputs, word_bits: int = 64) -> bool:
+    ins = _u64(inputs)
+    outs = _u64(outputs)
+    S, k = ins.shape
+    return bool(lib().orc_ext_check(postfix.encode(), len(postfix), word_bits, k, S,
+                                    _p(ins), _p(outs)))
+
+
+def ext_search(inputs, outputs, max_size: int, word_bits: int = 64, include_edges: bool = False,
+               n_threads: int = 0) -> dict:
+    ins = _u64(inputs)
+    outs = _u64(outputs)
+    S, k = ins.shape
+    res = OrcResult()
+    rc = lib().orc_ext_search(word_bits, k, S, _p(ins), _p(outs), max_size, int(include_edges),
+                              n_threads, C.byref(res))
+    if rc < 0:
+        raise ValueError(f"oracle ext search failed ({rc})")
+    return {"found": bool(res.found), "size": res.size, "op": res.op, "rank": res.rank,
+            "postfix": res.postfix[: res.size].decode() if res.found else "",
+            "candidates": res.candidates, "per_size": list(res.per_size)}
+
+
+def ext_vfb(inputs, outputs, max_len: int, word_bits: int = 64, cap_rows: int = 0) -> dict:
+    ins = _u64(inputs)
+    outs = _u64(outputs)
+    S, k = ins.shape
+    res = OrcVfbResult()
+    rc = lib().orc_ext_vfb(word_bits, k, S, _p(ins), _p(outs), max_len, cap_rows, C.byref(res))
+    if rc < 0:
+        raise ValueError(f"oracle ext vfb failed ({rc})")
+    return {"found": bool(res.found), "size": res.size, "op": res.op,
+            "postfix": res.postfix.decode() if res.found else "",
+            "cache_full": bool(res.cache_full), "candidates": res.candidates,
+            "rows_per_size": list(res.rows_per_size), "rows_total": res.rows_total}

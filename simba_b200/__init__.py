@@ -44,7 +44,7 @@ class _Options(C.Structure):
                 ("table_bytes", C.c_int64), ("stream", C.c_uint64),
                 ("vfb_cache_rows", C.c_int64), ("vfb_reference_dedup", C.c_int32),
                 ("unit_log2", C.c_int32), ("class_prior", C.POINTER(C.c_float)),
-                ("rank_order", C.c_int32), ("reserved", C.c_int32)]
+                ("rank_order", C.c_int32), ("grammar", C.c_int32)]
 
 
 class _BatchResult(C.Structure):
@@ -82,7 +82,10 @@ class _Result(C.Structure):
                 ("expr", C.c_char * 512), ("seconds", C.c_double), ("device_ms", C.c_double),
                 ("candidates", C.c_uint64), ("evaluated", C.c_uint64),
                 ("per_size", C.c_uint64 * 33), ("max_size_searched", C.c_int32),
-                ("launches", C.c_int32), ("kernel_ms", C.c_double), ("alg_ops", C.c_uint64)]
+                ("launches", C.c_int32), ("kernel_ms", C.c_double), ("alg_ops", C.c_uint64),
+                ("join_ms", C.c_double), ("nested_ms", C.c_double),
+                ("join_candidates", C.c_uint64), ("nested_candidates", C.c_uint64),
+                ("join_bytes_streamed", C.c_double), ("join_table_bytes", C.c_double)]
 
 
 _lib = None
@@ -144,6 +147,12 @@ class Result:
     launches: int = 0
     kernel_ms: float = 0.0
     alg_ops: int = 0
+    join_ms: float = 0.0
+    nested_ms: float = 0.0
+    join_candidates: int = 0
+    nested_candidates: int = 0
+    join_bytes_streamed: float = 0.0
+    join_table_bytes: float = 0.0
 
     @property
     def found(self) -> bool:
@@ -153,7 +162,9 @@ class Result:
 def _res(r: _Result) -> Result:
     return Result(r.status, r.size, r.op, r.rank, r.postfix.decode(), r.expr.decode(),
                   r.seconds, r.device_ms, r.candidates, r.evaluated, list(r.per_size),
-                  r.table_size, r.max_size_searched, r.launches, r.kernel_ms, r.alg_ops)
+                  r.table_size, r.max_size_searched, r.launches, r.kernel_ms, r.alg_ops,
+                  r.join_ms, r.nested_ms, r.join_candidates, r.nested_candidates,
+                  r.join_bytes_streamed, r.join_table_bytes)
 
 
 class _Arrays:
@@ -170,7 +181,7 @@ class _Arrays:
 
 def _opts(device=0, complete=False, verbose=False, naive=False, budget=0.0,
           table_bytes=0, stream=0, cache_rows=0, reference_dedup=False,
-          unit_log2=0, class_prior=None, rtid=False) -> _Options:
+          unit_log2=0, class_prior=None, rtid=False, extended=False) -> _Options:
     o = _Options()
     o.device = device
     o.size_range = 1 if complete else 0
@@ -183,6 +194,7 @@ def _opts(device=0, complete=False, verbose=False, naive=False, budget=0.0,
     o.vfb_reference_dedup = 1 if reference_dedup else 0
     o.unit_log2 = int(unit_log2)
     o.rank_order = 1 if rtid else 0
+    o.grammar = 1 if extended else 0
     if class_prior is not None:  # the caller keeps the array alive for the call
         o.class_prior = class_prior.ctypes.data_as(C.POINTER(C.c_float))
     return o
@@ -195,7 +207,8 @@ def _check(rc: int) -> None:
 
 
 def solve(inst: Instance, max_size: int, **kw) -> Result:
-    """Plain SIMBA search (the reference's NoCache::solve, simba/src/nocache.cu:197-289)."""
+    """Plain SIMBA search (the reference's NoCache::solve, simba/src/nocache.cu:197-289).
+    extended=True searches the extended grammar ~ & | ^ << >> neg + - * / %."""
     a = _Arrays(inst)
     r = _Result()
     rc = lib().simba_solve(C.byref(a.c), max_size, C.byref(_opts(**kw)), C.byref(r))
@@ -342,9 +355,12 @@ def rank_of(postfix: str, n_terms: int) -> int:
     return r.value
 
 
-def format_postfix(postfix: str, style: str = "simba") -> str:
+def format_postfix(postfix: str, style: str = "simba", extended: bool = False) -> str:
+    """Infix form in the SIMBA or VFB syntax; `extended` reads '<' '>' '/' '%'
+    as the extended grammar's << >> / %."""
     buf = C.create_string_buffer(4096)
-    _check(lib().simba_format(postfix.encode(), 0 if style == "simba" else 1, buf, 4096))
+    code = (0 if style == "simba" else 1) + (2 if extended else 0)
+    _check(lib().simba_format(postfix.encode(), code, buf, 4096))
     return buf.value.decode()
 
 

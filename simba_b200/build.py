@@ -35,9 +35,10 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas"
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", f"-I{CUDA_HOME / 'include'}"]
 
 CU_SOURCES = ["search_u64.cu", "search_u32.cu", "search_static.cu", "peak.cu", "vfb.cu",
-              "mlp.cu"]
+              "mlp.cu", "ext.cu"]
 CPP_SOURCES = ["capi.cpp"]
-HEADERS = ["grammar.h", "engine.h", "cuda_util.h", "json_lite.h", "search_impl.cuh"]
+HEADERS = ["grammar.h", "ext_grammar.h", "engine.h", "cuda_util.h", "json_lite.h",
+           "search_impl.cuh"]
 
 
 def _host_cxx() -> str:

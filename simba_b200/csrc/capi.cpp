@@ -12,6 +12,7 @@
 #include "../../include/simba_b200.h"
 #include "engine.h"
 #include "grammar.h"
+#include "ext_grammar.h"
 #include "json_lite.h"
 
 namespace simba {
@@ -87,10 +88,11 @@ bool host_check(const std::string& p, const HostInstance& h) {
 
 // SIMBA style: MBAToString, simba/src/nocache.cu:162-195.
 // VFB style: toString, vfb/src/full-cache.cu:483-509.
-std::string format_postfix(const std::string& p, int style) {
+// grammar 1: '<' '>' '/' '%' are the operators << >> / % (ext_grammar.h).
+std::string format_postfix(const std::string& p, int style, int grammar) {
   std::vector<std::string> st;
   for (char c : p) {
-    int op = char_op(c);
+    int op = grammar == 1 ? ext_char_code(c) : char_op(c);
     if (op < 0) {
       st.push_back("v" + std::to_string(c - '0'));
     } else if (is_unary(op)) {
@@ -105,7 +107,8 @@ std::string format_postfix(const std::string& p, int style) {
       st.pop_back();
       std::string l = st.back();
       st.pop_back();
-      st.push_back(style == 0 ? "(" + l + " " + c + " " + r + ")" : "(" + l + ")" + c + "(" + r + ")");
+      const std::string sym = c == '<' && op == OP_SHL ? "<<" : (c == '>' && op == OP_SHR ? ">>" : std::string(1, c));
+      st.push_back(style == 0 ? "(" + l + " " + sym + " " + r + ")" : "(" + l + ")" + sym + "(" + r + ")");
     }
   }
   return st.size() == 1 ? st[0] : "";
@@ -145,11 +148,12 @@ static EngineOptions to_opts(const simba_options* o) {
     e.unit_log2 = o->unit_log2;
     e.class_prior = o->class_prior;
     e.rank_order = o->rank_order;
+    e.grammar = o->grammar;
   }
   return e;
 }
 
-static void fill_result(const SolveOutcome& oc, double secs, simba_result* r) {
+static void fill_result(const SolveOutcome& oc, double secs, simba_result* r, int grammar = 0) {
   memset(r, 0, sizeof(*r));
   r->status = oc.status;
   r->size = oc.size;
@@ -158,7 +162,7 @@ static void fill_result(const SolveOutcome& oc, double secs, simba_result* r) {
   r->table_size = oc.table_size;
   snprintf(r->postfix, sizeof(r->postfix), "%s", oc.postfix.c_str());
   if (oc.status == SIMBA_OK) {
-    std::string e = format_postfix(oc.postfix, 0);
+    std::string e = format_postfix(oc.postfix, 0, grammar);
     snprintf(r->expr, sizeof(r->expr), "%s", e.c_str());
   } else {
     snprintf(r->expr, sizeof(r->expr), "Not found !");
@@ -172,6 +176,12 @@ static void fill_result(const SolveOutcome& oc, double secs, simba_result* r) {
   r->launches = oc.launches;
   r->kernel_ms = oc.kernel_ms;
   r->alg_ops = oc.alg_ops;
+  r->join_ms = oc.join_ms;
+  r->nested_ms = oc.nested_ms;
+  r->join_candidates = oc.join_candidates;
+  r->nested_candidates = oc.nested_candidates;
+  r->join_bytes_streamed = oc.join_bytes_streamed;
+  r->join_table_bytes = oc.join_table_bytes;
 }
 
 int read_instance_json(const std::string& path, HostInstance* h) {
@@ -264,6 +274,13 @@ struct simba_session {
   HostInstance h;
 };
 
+// The extended grammar is an option of simba_solve and vfb_solve only.
+static bool grammar_unsupported(const simba_options* opt) {
+  if (!opt || opt->grammar == 0) return false;
+  set_last_error("grammar 1 (extended) is supported by simba_solve and vfb_solve only");
+  return true;
+}
+
 extern "C" {
 
 int simba_solve(const simba_instance* inst, int max_size, const simba_options* opt,
@@ -283,6 +300,28 @@ int simba_solve(const simba_instance* inst, int max_size, const simba_options* o
     set_last_error("rank_order must be 0, or 1 for the plain spine search");
     result->status = SIMBA_E_ARG;
     return SIMBA_E_ARG;
+  }
+  if (opt && (opt->grammar < 0 || opt->grammar > 1)) {
+    set_last_error("grammar must be 0 (reference) or 1 (extended)");
+    result->status = SIMBA_E_ARG;
+    return SIMBA_E_ARG;
+  }
+  if (opt && opt->grammar == 1) {
+    if (opt->rank_order != 0 || opt->class_prior) {
+      set_last_error("the extended grammar runs the plain rank order only");
+      result->status = SIMBA_E_ARG;
+      return SIMBA_E_ARG;
+    }
+    SolveOutcome oc;
+    rc = ext_solve(h, max_size, to_opts(opt), &oc);
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (rc < 0) {
+      memset(result, 0, sizeof(*result));
+      result->status = rc;
+      return rc;
+    }
+    fill_result(oc, secs, result, 1);
+    return result->status;
   }
   SearchSession* s = nullptr;
   rc = make_search_session(h, to_opts(opt), &s);
@@ -319,6 +358,15 @@ int simba_solve_noalloc(const simba_instance* inst, int max_size, const simba_op
     result->status = SIMBA_E_ARG;
     return SIMBA_E_ARG;
   }
+  if (opt && (opt->engine != 0 || opt->class_prior)) {
+    set_last_error("simba_solve_noalloc runs the plain spine search only (engine 0, no class_prior)");
+    result->status = SIMBA_E_ARG;
+    return SIMBA_E_ARG;
+  }
+  if (grammar_unsupported(opt)) {
+    result->status = SIMBA_E_ARG;
+    return SIMBA_E_ARG;
+  }
   SolveOutcome oc;
   rc = solve_static(h, max_size, to_opts(opt), &oc);
   const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -333,6 +381,7 @@ int simba_solve_noalloc(const simba_instance* inst, int max_size, const simba_op
 int simba_solve_batch(const simba_instance* insts, int n, const int max_size_arg,
                       const simba_options* opt, simba_batch_result* results, simba_batch_stats* stats) {
   if (!insts || n < 0 || !results) return SIMBA_E_ARG;
+  if (grammar_unsupported(opt)) return SIMBA_E_ARG;
   if (opt && opt->rank_order != 0) {
     set_last_error("rank_order 1 (RTid) is supported by simba_solve only");
     return SIMBA_E_ARG;
@@ -379,6 +428,7 @@ int simba_session_create(const simba_instance* inst, const simba_options* opt,
                          simba_session** session) {
   if (!session) return SIMBA_E_ARG;
   *session = nullptr;
+  if (grammar_unsupported(opt)) return SIMBA_E_ARG;
   if (opt && opt->rank_order != 0) {
     set_last_error("rank_order 1 (RTid) is supported by simba_solve only");
     return SIMBA_E_ARG;
@@ -436,6 +486,12 @@ int vfb_solve(const simba_instance* inst, int max_len, const simba_options* opt,
     result->status = rc;
     return rc;
   }
+  if (opt && (opt->grammar < 0 || opt->grammar > 1 ||
+              (opt->grammar == 1 && opt->vfb_reference_dedup))) {
+    set_last_error("grammar must be 0, or 1 (extended) without vfb_reference_dedup");
+    result->status = SIMBA_E_ARG;
+    return SIMBA_E_ARG;
+  }
   VfbOutcome oc;
   rc = vfb_run(h, max_len, to_opts(opt), opt ? opt->vfb_reference_dedup : 0,
                opt ? opt->vfb_cache_rows : 0, &oc);
@@ -450,7 +506,7 @@ int vfb_solve(const simba_instance* inst, int max_len, const simba_options* opt,
   result->max_size_searched = oc.max_size_searched;
   snprintf(result->postfix, sizeof(result->postfix), "%s", oc.postfix.c_str());
   if (oc.status == SIMBA_OK) {
-    const std::string e = format_postfix(oc.postfix, 1);
+    const std::string e = format_postfix(oc.postfix, 1, opt ? opt->grammar : 0);
     snprintf(result->expr, sizeof(result->expr), "%s", e.c_str());
   } else {
     snprintf(result->expr, sizeof(result->expr), "Not found !");
@@ -523,7 +579,7 @@ int simba_rank_of(const char* postfix, int n_terms, uint64_t* rank) {
 
 int simba_format(const char* postfix, int style, char* out, int cap) {
   if (!postfix || !out || cap <= 0) return SIMBA_E_ARG;
-  const std::string s = format_postfix(postfix, style);
+  const std::string s = format_postfix(postfix, style & 1, (style >> 1) & 1);
   if (s.empty()) return SIMBA_E_ARG;
   if ((int)s.size() + 1 > cap) return SIMBA_E_ARG;
   memcpy(out, s.c_str(), s.size() + 1);

@@ -1,5 +1,6 @@
 // Internal C++ interface between the C ABI (capi.cpp) and the CUDA engines
-// (search.cu, vfb.cu, batch.cu).  Nothing here crosses the library boundary.
+// (search_impl.cuh via search_u32.cu / search_u64.cu, search_static.cu,
+// vfb.cu, mlp.cu).  Nothing here crosses the library boundary.
 #pragma once
 #include <cstdint>
 #include <string>
@@ -32,6 +33,7 @@ struct EngineOptions {
   int unit_log2 = 0;         // log2 candidates per work unit, 0 = 22
   const float* class_prior = nullptr;  // guided search: 64 shape-class priors
   int rank_order = 0;        // 0 rank order, 1 RTid order (single-instance solve only)
+  int grammar = 0;           // 0 the reference grammar, 1 extended (ext_grammar.h)
 };
 
 // Per-solve outcome filled by the engines (capi.cpp formats the strings).
@@ -50,6 +52,10 @@ struct SolveOutcome {
   int launches = 0;
   double kernel_ms = 0.0;
   uint64_t alg_ops = 0;
+  // the two launch kinds of the spine kernel (single-instance searches)
+  double join_ms = 0.0, nested_ms = 0.0;
+  uint64_t join_candidates = 0, nested_candidates = 0;
+  double join_bytes_streamed = 0.0, join_table_bytes = 0.0;
 };
 
 std::string last_error();
@@ -83,6 +89,13 @@ class SearchSession {
 
 int make_search_session(const HostInstance& h, const EngineOptions& o,
                         SearchSession** out);
+
+// Plain search in the extended grammar (ext.cu) and its host re-check.
+int ext_solve(const HostInstance& h, int max_size, const EngineOptions& o, SolveOutcome* out);
+bool ext_check_host(const std::string& postfix, const HostInstance& h);
+// The same check with VFB's whole-vector rule for / and % (a divisor vector
+// with a zero element yields the dividend vector).
+bool ext_vector_check(const std::string& postfix, const HostInstance& h);
 
 // Plain search with all scratch in a static __device__ array (search_static.cu).
 int solve_static(const HostInstance& h, int max_size, const EngineOptions& o, SolveOutcome* out);
@@ -149,8 +162,9 @@ struct VfbOutcome {
 int vfb_run(const HostInstance& h, int max_len, const EngineOptions& o, int inverted,
             int64_t cache_rows, VfbOutcome* out);
 
-// Format a postfix string in the SIMBA (style 0) or VFB (style 1) syntax.
-std::string format_postfix(const std::string& postfix, int style);
+// Format a postfix string in the SIMBA (style 0) or VFB (style 1) syntax;
+// grammar 1 reads '<' '>' '/' '%' as the extended operators.
+std::string format_postfix(const std::string& postfix, int style, int grammar = 0);
 
 // Host-side exact check of an expression on every sample.
 bool host_check(const std::string& postfix, const HostInstance& h);

@@ -59,7 +59,8 @@ constexpr int kMaxDepth = 12;  // spine levels
 constexpr int kThreads = 256;  // CTA size of the search kernels
 constexpr int kQueue = 128;    // shared-memory queue of matches to verify
 constexpr int kPre = 256;      // shared-memory queue of sample-0 matches to filter
-constexpr int kPreG = 262144;  // the same queue per CTA in global memory, when given
+constexpr int kPreG = 131072;  // the same queue per CTA in global memory, when given
+                               // (8-byte entries: context << 32 | bottom index)
 // Tuning knobs (compile-time): contexts per thread, minimum resident CTAs
 // per SM.
 #ifndef SIMBA_KR
@@ -207,7 +208,7 @@ struct Params {
   unsigned long long* start_ns;
   int* flags;  // [0] budget expired, [1] inversion failure, [2] queue overflows
   unsigned long long* hits;  // sample-0 matches sent to verification (may be null)
-  unsigned long long* preq;  // per-CTA queues of sample-0 matches, [grid][kPreG][2] (may be null)
+  unsigned long long* preq;  // per-CTA queues of sample-0 matches, [grid][kPreG] (may be null)
   unsigned join_off;         // byte offset of JoinSmem in dynamic shared memory; 0: no join units
   unsigned long long total_units;
   unsigned long long unit_offset;  // this shard's first unit (multi-GPU)
@@ -563,15 +564,17 @@ template <class W>
 __device__ __forceinline__ void pre_push(const Params<W>& p, const InstDesc<W>& d, Smem& sm, const Item& it,
                                          unsigned long long c, unsigned long long v, const W* s_in,
                                          const W* s_out) {
-  const int i = atomicAdd(&sm.pn, 1);
   if (p.preq) {
-    if (i < kPreG) {
-      unsigned long long* e = p.preq + ((size_t)blockIdx.x * kPreG + i) * 2;
-      e[0] = c;
-      e[1] = v;
-      return;
+    // a context or bottom index beyond 32 bits (deep spines, huge tables)
+    // skips the queue and goes straight to verification
+    if ((c >> 32) == 0 && (v >> 32) == 0) {
+      const int i = atomicAdd(&sm.pn, 1);
+      if (i < kPreG) {
+        p.preq[(size_t)blockIdx.x * kPreG + i] = c << 32 | v;
+        return;
+      }
     }
-  } else if (i < kPre) {
+  } else if (const int i = atomicAdd(&sm.pn, 1); i < kPre) {
     sm.pre_c[i] = c;
     sm.pre_v[i] = v;
     return;
@@ -586,10 +589,10 @@ __device__ void filter_queue(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
                              const W* s_out) {
   const int n = min(sm.pn, p.preq ? kPreG : kPre);
   const Item& it = sm.item;
-  const unsigned long long* gq = p.preq ? p.preq + (size_t)blockIdx.x * kPreG * 2 : nullptr;
+  const unsigned long long* gq = p.preq ? p.preq + (size_t)blockIdx.x * kPreG : nullptr;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const unsigned long long c = gq ? gq[2 * i] : sm.pre_c[i];
-    const unsigned long long v = gq ? gq[2 * i + 1] : sm.pre_v[i];
+    const unsigned long long c = gq ? gq[i] >> 32 : sm.pre_c[i];
+    const unsigned long long v = gq ? gq[i] & 0xFFFFFFFFULL : sm.pre_v[i];
     bool pass;
     if (it.fused) {
       const Ctx<W> cx = p.ctxs[it.ctx_off + c];
@@ -655,6 +658,22 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
   const unsigned long long q0 = v0 / VW, q1 = (v1 + VW - 1) / VW;
   const uint4* V4 = reinterpret_cast<const uint4*>(V);
 
+  // First pass on the low 32 bits only (64-bit words): the low half of every
+  // level's result (bitwise operators, +, -, *, x -> +-x + c) depends only on
+  // the low halves of its operands, so a candidate whose low halves fail the
+  // masked compare cannot match.  The rare survivors are compared in full.
+  using H = unsigned;
+  Explicit<H> XH;
+  if (E > 0) {
+#pragma unroll
+    for (int j = 0; j < EE; ++j) {
+      XH.kind[j] = X.kind[j];
+      XH.op[j] = X.op[j];
+      XH.sl[j] = X.sl[j];
+      XH.eps[j] = X.eps[j];
+      XH.c[j] = (H)X.c[j];
+    }
+  }
   auto test = [&](const uint4& raw, unsigned long long q) {
     W xs[VW];
     memcpy(xs, &raw, 16);
@@ -663,9 +682,14 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
     for (int e = 0; e < VW; ++e) {
 #pragma unroll
       for (int r = 0; r < kR; ++r) {
-        W y = xs[e];
-        if (E > 0) y = eval_explicit<W, E>(X, WX[r], y);
-        hit |= FULL ? (y == K[r]) : ((W)(y & M[r]) == K[r]);
+        H y = (H)xs[e];
+        if (E > 0) {
+          H wh[EE];
+#pragma unroll
+          for (int j = 0; j < EE; ++j) wh[j] = (H)WX[r][j];
+          y = eval_explicit<H, E>(XH, wh, y);
+        }
+        hit |= FULL ? (y == (H)K[r]) : ((H)(y & (H)M[r]) == (H)K[r]);
       }
     }
     if (!hit) return;
@@ -1499,7 +1523,11 @@ static inline void fuse_small(std::vector<Item>& items, std::vector<Item>* small
     }
     size_t gi = 0;
     for (; gi < groups.size(); ++gi)
-      if (groups[gi].bottom == it.bottom && groups[gi].full == it.full &&
+      // joinable spines of one bottom share a group whatever their mask kind
+      // (the join reads each context's own mask), so the bottom table is
+      // streamed once per block of contexts instead of once per kind
+      if (groups[gi].bottom == it.bottom &&
+          (groups[gi].full == it.full || (it.joinable && groups[gi].joinable)) &&
           groups[gi].joinable == it.joinable &&
           (!by_prio || groups[gi].prio == it.prio))
         break;
@@ -1558,6 +1586,7 @@ class Search final : public SearchSession {
     if (ev0_) cudaEventDestroy(ev0_);
     if (evk_) cudaEventDestroy(evk_);
     if (ev1_) cudaEventDestroy(ev1_);
+    if (evj_) cudaEventDestroy(evj_);
   }
 
   int init() {
@@ -1572,6 +1601,7 @@ class Search final : public SearchSession {
     SB_CUDA(cudaEventCreate(&ev0_));
     SB_CUDA(cudaEventCreate(&evk_));
     SB_CUDA(cudaEventCreate(&ev1_));
+    SB_CUDA(cudaEventCreate(&evj_));
     SB_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, o_.device));
     mask_ = h_.bits == 64 ? ~0ULL : 0xFFFFFFFFULL;
     // count table up to the largest size whose counts fit in 64 bits
@@ -1630,7 +1660,7 @@ class Search final : public SearchSession {
     int occj = 1;
     SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occj, spine_kernel<W>, kThreads, smem_join_));
     grid_join_ = sms_ * std::max(occj, 1);
-    SB_CUDA(d_preq_.reserve((size_t)std::max(grid_, grid_join_) * kPreG * 16));
+    SB_CUDA(d_preq_.reserve((size_t)std::max(grid_, grid_join_) * kPreG * 8));
     int occn = 1;
     SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occn, naive_kernel<W>, kThreads, smem_bytes_));
     grid_naive_ = sms_ * std::max(occn, 1);
@@ -1837,6 +1867,23 @@ class Search final : public SearchSession {
       SB_CUDA(cudaMemcpyAsync(d_items_.p, items.data(), items.size() * sizeof(Item),
                               cudaMemcpyHostToDevice, stream_));
       for (auto& it : items) alg_total += item_alg_ops(it, sizeof(W));
+      {  // planned work of the two launch kinds
+        bool seen[kMaxSize + 1] = {};
+        for (size_t q = 0; q < items.size(); ++q) {
+          const Item& it = items[q];
+          const double c = (double)it.nctx * (double)it.nv;
+          if (q >= nj) {
+            nested_cand_ += c;
+            continue;
+          }
+          join_cand_ += c;
+          join_streamed_ += (double)it.nv * sizeof(W) * (double)it.cblocks;
+          if (!seen[(int)it.bottom]) {
+            seen[(int)it.bottom] = true;
+            join_table_ += (double)it.nv * sizeof(W);
+          }
+        }
+      }
       Params<W> p = params(s);
       p.items = d_items_.as<Item>() + nj;
       p.nitems = (int)(items.size() - nj);
@@ -1867,6 +1914,7 @@ class Search final : public SearchSession {
         spine_kernel<W><<<grid_join_, kThreads, smem_join_, stream_>>>(pj);
         ++launches_;
       }
+      SB_CUDA(cudaEventRecord(evj_, stream_));
       if (nj < items.size()) {
         p.counter = d_scal_.as<unsigned long long>() + 7;  // zeroed with the flags
         spine_kernel<W><<<grid_, kThreads, smem_bytes_, stream_>>>(p);
@@ -1878,6 +1926,8 @@ class Search final : public SearchSession {
       p.stop_on_match = stop ? 1 : 0;
       alg_total = (double)ct_.n[s][8] * (double)s * (sizeof(W) == 8 ? 2.0 : 1.0);
       SB_CUDA(cudaEventRecord(evk_, stream_));
+      SB_CUDA(cudaEventRecord(evj_, stream_));  // no join launch
+      nested_cand_ += (double)ct_.n[s][8];
       const unsigned __int128 n = ct_.n[s][8];
       const uint64_t lo = (uint64_t)(n * (unsigned)shard / (unsigned)nshards);
       const uint64_t hi = (uint64_t)(n * (unsigned)(shard + 1) / (unsigned)nshards);
@@ -1888,11 +1938,14 @@ class Search final : public SearchSession {
     SB_CUDA(cudaEventRecord(ev1_, stream_));
     SB_CUDA(cudaMemcpyAsync(h_scal_, d_scal_.p, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_));
     SB_CUDA(cudaStreamSynchronize(stream_));
-    float e = 0, ek = 0;
+    float e = 0, ek = 0, ej = 0;
     SB_CUDA(cudaEventElapsedTime(&e, ev0_, ev1_));
     SB_CUDA(cudaEventElapsedTime(&ek, evk_, ev1_));
+    SB_CUDA(cudaEventElapsedTime(&ej, evk_, evj_));
     *ms += e;
     kernel_ms_ += ek;
+    join_ms_ += ej;
+    nested_ms_ += ek - ej;
     const unsigned long long* hs = static_cast<unsigned long long*>(h_scal_);
     *best = hs[1];
     *evaluated += hs[2];
@@ -1931,6 +1984,7 @@ class Search final : public SearchSession {
     }
     launches_ = 0;
     kernel_ms_ = 0.0;
+    join_ms_ = nested_ms_ = join_cand_ = nested_cand_ = join_streamed_ = join_table_ = 0.0;
     alg_ops_ = 0;
     stamp_start_kernel<<<1, 1, 0, stream_>>>(d_scal_.as<unsigned long long>() + 3);
     ++launches_;
@@ -1949,6 +2003,12 @@ class Search final : public SearchSession {
       if (best != ~0ULL && o_.rank_order == 1 && s > 1) best = rtid_rank(ct_.n, s, best);
       out->launches = launches_;
       out->kernel_ms = kernel_ms_;
+      out->join_ms = join_ms_;
+      out->nested_ms = nested_ms_;
+      out->join_candidates = (uint64_t)join_cand_;
+      out->nested_candidates = (uint64_t)nested_cand_;
+      out->join_bytes_streamed = join_streamed_;
+      out->join_table_bytes = join_table_;
       out->alg_ops = alg_ops_;
       out->max_size_searched = s;
       out->table_size = std::max(out->table_size, last_T_);
@@ -2003,10 +2063,12 @@ class Search final : public SearchSession {
   int count_ok_max_ = 0;
   uint64_t mask_ = 0;
   cudaStream_t stream_ = nullptr;
-  cudaEvent_t ev0_ = nullptr, evk_ = nullptr, ev1_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, evk_ = nullptr, ev1_ = nullptr, evj_ = nullptr;
   bool own_stream_ = true;
   int launches_ = 0;
   double kernel_ms_ = 0.0;
+  double join_ms_ = 0.0, nested_ms_ = 0.0, join_cand_ = 0.0, nested_cand_ = 0.0;
+  double join_streamed_ = 0.0, join_table_ = 0.0;
   uint64_t alg_ops_ = 0;
   int sms_ = 0, grid_ = 0, grid_naive_ = 0, grid_join_ = 0;
   size_t smem_bytes_ = 0, join_off_ = 0, smem_join_ = 0;
@@ -2197,7 +2259,7 @@ class Batch {
     int occ = 1;
     SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, spine_kernel<W>, kThreads, smem));
     const int grid = sms * std::max(occ, 1);
-    SB_CUDA(d_preq_.reserve((size_t)grid * kPreG * 16));
+    SB_CUDA(d_preq_.reserve((size_t)grid * kPreG * 8));
     SB_CUDA(d_ns_.reserve((size_t)n * 16 + 16));
     SB_CUDA(cudaMemsetAsync(d_ns_.p, 0, (size_t)n * 16, stream_));
     std::vector<unsigned long long> ns(2 * (size_t)n + 2);

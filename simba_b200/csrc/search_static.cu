@@ -18,7 +18,12 @@
 //    on the GPU (other host threads, other streams) race on it: serialise
 //    them.
 //  * No stream or event is created: the search runs on options.stream (0 =
-//    the default stream) and is timed with the host clock.
+//    the legacy default stream) and is timed with the host clock.  While
+//    another stream is being captured, pass a non-blocking stream: work on
+//    the legacy default stream synchronises with blocking streams and would
+//    break that capture.
+//  * The looked-up address is cached per device ordinal; it is not valid
+//    after cudaDeviceReset destroys the context that holds the array.
 //  * Sizes whose value tables or spine list do not fit the array are
 //    rejected with SIMBA_E_ARG and a message naming the limit.
 #include <cuda_runtime.h>

@@ -10,12 +10,14 @@
 //  * One kernel per (size, operator, split) block; a candidate's vector is
 //    computed element by element from the two operand rows and folded into a
 //    64-bit fingerprint A plus a 32-bit check B on the fly -- never stored.
-//  * Open-addressing hash table (linear probing, power-of-two capacity,
-//    64-bit keys, CAS insert).  A key hit whose published check B differs is
-//    a fingerprint collision and probing continues, so two different vectors
-//    are merged only if both A and B collide.
-//  * A new vector is recomputed, appended with an atomic row counter (no
-//    separate compaction pass) and compared with the target.
+//  * Open-addressing hash table (linear probing from a multiplicative mix of
+//    A, power-of-two capacity, 64-bit keys, CAS insert).  Dedup is exact: the
+//    thread that claims a slot appends its vector with an atomic row counter
+//    (no separate compaction pass) and then publishes the row index in the
+//    slot; a thread whose fingerprint hits the slot waits for that
+//    publication (bounded) and compares its vector with the stored row
+//    element by element, so two different vectors are never merged, whatever
+//    their fingerprints.  New vectors are compared with the target.
 //  * Kernels of a size run back to back on one stream; each one exits at
 //    once if an earlier kernel already found the target, so the host
 //    synchronises once per size instead of after every chunk.
@@ -23,7 +25,13 @@
 // vector is stored when the hash set already held it and dropped on a fresh
 // insert (warpcore HashSet::insert returns i+1 > 0 for a present key,
 // vfb/include/warpcore/hash_set.cuh:210-214,230-233, and the caller keeps
-// `insert(...) > 0`, full-cache.cu:285-286).
+// `insert(...) > 0`, full-cache.cu:285-286).  The first occurrence of a
+// vector is then never stored, so this mode keeps the reference's
+// fingerprint-only test (here 64-bit A plus a 32-bit check B) instead of
+// the exact comparison.
+// SIMBA_VFB_FP_BITS=b (1..63, tests only) keeps b bits of A, which forces
+// fingerprint collisions; the exact mode must still store every distinct
+// vector once.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,6 +45,7 @@
 #include "cuda_util.h"
 #include "engine.h"
 #include "grammar.h"
+#include "ext_grammar.h"
 
 namespace simba {
 
@@ -49,8 +58,11 @@ struct VfbArgs {
   uint32_t* rl;               //             left operand row
   uint32_t* rr;               //             right operand row
   unsigned long long* keys;   // hash keys (fingerprint A), kEmptyKey = free
-  unsigned* vals;             // hash check B (0 = not yet published)
+  unsigned* vals;             // exact mode: stored row + 1 (0 = not yet published,
+                              // kNoRow = the cache was full); reference mode: check B
   unsigned long long mask;    // hash capacity - 1
+  int shift;                  // 64 - log2(hash capacity): start slot of a key
+  unsigned long long fp_mask; // bits of A kept (all but in collision tests)
   unsigned long long* nrows;  // row counter
   unsigned long long cap;     // row capacity
   const W* target;            // S words
@@ -64,8 +76,11 @@ struct VfbArgs {
   int launch;                 // id of this launch within the search
 };
 
+// One element of a composed vector.  z (division and modulo only): the
+// divisor vector holds a zero somewhere, and the result is the dividend
+// vector (full-cache.cu:230-256); otherwise every divisor element is nonzero.
 template <class W, int OP>
-__device__ __forceinline__ W vop(W l, W r) {
+__device__ __forceinline__ W vop(W l, W r, bool z = false) {
   if (OP == OP_NOT) return (W)~l;
   if (OP == OP_NEG) return (W)(W(0) - l);
   if (OP == OP_AND) return l & r;
@@ -73,7 +88,11 @@ __device__ __forceinline__ W vop(W l, W r) {
   if (OP == OP_XOR) return l ^ r;
   if (OP == OP_ADD) return (W)(l + r);
   if (OP == OP_SUB) return (W)(l - r);
-  return (W)(l * r);
+  if (OP == OP_MUL) return (W)(l * r);
+  if (OP == OP_SHL) return r >= (W)(8 * sizeof(W)) ? W(0) : (W)(l << r);
+  if (OP == OP_SHR) return r >= (W)(8 * sizeof(W)) ? W(0) : (W)(l >> r);
+  if (OP == OP_DIV) return z ? l : (W)(l / r);
+  return z ? l : (W)(l % r);  // OP_MOD
 }
 
 // Fingerprint: A is a multiply-xorshift fold finished with the MurmurHash3
@@ -102,11 +121,20 @@ __device__ __forceinline__ unsigned fp_check(unsigned long long b) {
 }
 
 enum { INS_NEW = 0, INS_DUP = 1, INS_FULL = 2 };
+constexpr unsigned kNoRow = 0xFFFFFFFFu;   // published by an insert that found the cache full
+constexpr int kPublishSpin = 1 << 20;      // polls of an unpublished slot before giving up
 
-__device__ int hash_insert(unsigned long long* keys, unsigned* vals, unsigned long long mask,
+__device__ __forceinline__ unsigned long long start_slot(unsigned long long A, int shift) {
+  return (A * 0x9E3779B97F4A7C15ULL) >> shift;
+}
+
+// Reference mode: fingerprint-only set semantics (a key hit whose published
+// check B differs is a collision and probing continues).
+__device__ int hash_insert(unsigned long long* keys, unsigned* vals, unsigned long long mask, int shift,
                            unsigned long long A, unsigned B) {
+  const unsigned long long s0 = start_slot(A, shift);
   for (unsigned long long p = 0; p <= mask; ++p) {
-    const unsigned long long s = (A + p) & mask;
+    const unsigned long long s = (s0 + p) & mask;
     unsigned long long k = keys[s];
     if (k == kEmptyKey) {
       const unsigned long long old = atomicCAS(&keys[s], kEmptyKey, A);
@@ -124,20 +152,70 @@ __device__ int hash_insert(unsigned long long* keys, unsigned* vals, unsigned lo
   return INS_FULL;
 }
 
+template <class W>
+__device__ __forceinline__ W load_cg(const W* p) {
+  if (sizeof(W) == 8) return (W)__ldcg(reinterpret_cast<const unsigned long long*>(p));
+  return (W)__ldcg(reinterpret_cast<const unsigned*>(p));
+}
+
+// Exact mode: claim a slot for key A (INS_NEW, *slot set: the caller stores
+// the vector and publishes its row), or find the vector already stored
+// (INS_DUP): every slot holding A is compared element by element with the
+// vector `elem` once its row is published.  INS_FULL: no free slot.  A
+// publication that does not come within kPublishSpin polls sets flags[2] and
+// reports a duplicate; the host turns that flag into an error.
+template <class W, class Elem>
+__device__ int hash_claim_exact(const VfbArgs<W>& a, unsigned long long A, Elem elem,
+                                unsigned long long* slot) {
+  const unsigned long long s0 = start_slot(A, a.shift);
+  for (unsigned long long p = 0; p <= a.mask; ++p) {
+    const unsigned long long s = (s0 + p) & a.mask;
+    unsigned long long k = a.keys[s];
+    if (k == kEmptyKey) {
+      const unsigned long long old = atomicCAS(&a.keys[s], kEmptyKey, A);
+      if (old == kEmptyKey) {
+        *slot = s;
+        return INS_NEW;
+      }
+      k = old;
+    }
+    if (k != A) continue;
+    unsigned v = *(volatile unsigned*)&a.vals[s];
+    for (int t = 0; v == 0; ++t) {
+      if (t == kPublishSpin) {
+        atomicOr(&a.flags[2], 1);
+        return INS_DUP;
+      }
+      __nanosleep(64);
+      v = *(volatile unsigned*)&a.vals[s];
+    }
+    if (v == kNoRow) return INS_DUP;  // not stored: the cache is full and the search ends here
+    __threadfence();                  // the row's words were written before the publication
+    const W* row = a.rows + (unsigned long long)(v - 1) * a.S;
+    bool same = true;
+    for (int i = 0; i < a.S && same; ++i) same = load_cg<W>(row + i) == elem(i);
+    if (same) return INS_DUP;
+    // the same fingerprint for another vector: keep probing
+  }
+  return INS_FULL;
+}
+
 // Keep / store one composed candidate (x, y) whose fingerprint is (A, B):
 // insert into the hash set, append the vector when it is kept, compare it
 // with the target.  `elem(i)` recomputes element i of the vector.
 template <class W, int OP, class Elem>
 __device__ __forceinline__ void vfb_offer(const VfbArgs<W>& a, unsigned long long x, unsigned long long y,
                                           unsigned long long A, unsigned B, Elem elem) {
-  const int ins = hash_insert(a.keys, a.vals, a.mask, A, B);
-  bool keep;
-  if (a.inverted) keep = ins != INS_NEW;  // INS_FULL is kept too, as in the reference
-  else {
+  A &= a.fp_mask;
+  unsigned long long slot = ~0ULL;
+  if (a.inverted) {
+    // INS_FULL is kept too, as in the reference
+    if (hash_insert(a.keys, a.vals, a.mask, a.shift, A, B) == INS_NEW) return;
+  } else {
+    const int ins = hash_claim_exact<W>(a, A, elem, &slot);
     if (ins == INS_FULL) atomicOr(&a.flags[1], 1);
-    keep = ins == INS_NEW;
+    if (ins != INS_NEW) return;
   }
-  if (!keep) return;
   const unsigned long long row = atomicAdd(a.nrows, 1ULL);
   bool match = true;
   W* out = row < a.cap ? a.rows + row * a.S : nullptr;
@@ -152,6 +230,10 @@ __device__ __forceinline__ void vfb_offer(const VfbArgs<W>& a, unsigned long lon
     a.rr[row] = (uint32_t)y;
   } else {
     atomicOr(&a.flags[0], 1);
+  }
+  if (slot != ~0ULL) {  // publish the stored row to threads waiting on the slot
+    __threadfence();
+    atomicExch(&a.vals[slot], out ? (unsigned)(row + 1) : kNoRow);
   }
   if (match) {
     atomicCAS(a.found, ~0ULL, (x << 32) | y);
@@ -185,13 +267,16 @@ __global__ void __launch_bounds__(256) vfb_compose_kernel(VfbArgs<W> a) {
     }
     const W* L = a.rows + x * S;
     const W* R = a.rows + y * S;
+    bool z = false;
+    if (OP == OP_DIV || OP == OP_MOD)
+      for (int i = 0; i < S && !z; ++i) z = R[i] == W(0);
     unsigned long long fa = 0x243F6A8885A308D3ULL, fb = 0;
     for (int i = 0; i < S; ++i) {
-      const W v = vop<W, OP>(L[i], unary ? W(0) : R[i]);
+      const W v = vop<W, OP>(L[i], unary ? W(0) : R[i], z);
       fp_step(fa, fb, (unsigned long long)v, i);
     }
     vfb_offer<W, OP>(a, x, y, fp_final(fa, S), fp_check(fb),
-                     [&](int i) { return vop<W, OP>(L[i], unary ? W(0) : R[i]); });
+                     [&](int i) { return vop<W, OP>(L[i], unary ? W(0) : R[i], z); });
   }
 }
 
@@ -252,7 +337,16 @@ __global__ void vfb_init_kernel(VfbArgs<W> a, int k) {
   const W* v = a.rows + (unsigned long long)j * a.S;
   unsigned long long fa = 0x243F6A8885A308D3ULL, fb = 0;
   for (int i = 0; i < a.S; ++i) fp_step(fa, fb, (unsigned long long)v[i], i);
-  hash_insert(a.keys, a.vals, a.mask, fp_final(fa, a.S), fp_check(fb));
+  const unsigned long long A = fp_final(fa, a.S) & a.fp_mask;
+  if (a.inverted) {
+    hash_insert(a.keys, a.vals, a.mask, a.shift, A, fp_check(fb));
+  } else {  // the variables' rows are in place already
+    unsigned long long slot;
+    if (hash_claim_exact<W>(a, A, [&](int i) { return v[i]; }, &slot) == INS_NEW) {
+      __threadfence();
+      atomicExch(&a.vals[slot], (unsigned)(j + 1));
+    }
+  }
   a.rop[j] = -1;
   a.rl[j] = (uint32_t)j;
   a.rr[j] = 0;
@@ -299,7 +393,11 @@ static void launch_compose(int op, int grid, cudaStream_t st, const VfbArgs<W>& 
     case OP_NEG: vfb_compose_kernel<W, OP_NEG><<<grid, 256, 0, st>>>(a); break;
     case OP_ADD: vfb_compose_kernel<W, OP_ADD><<<grid, 256, 0, st>>>(a); break;
     case OP_SUB: vfb_compose_kernel<W, OP_SUB><<<grid, 256, 0, st>>>(a); break;
-    default: vfb_compose_kernel<W, OP_MUL><<<grid, 256, 0, st>>>(a); break;
+    case OP_MUL: vfb_compose_kernel<W, OP_MUL><<<grid, 256, 0, st>>>(a); break;
+    case OP_SHL: vfb_compose_kernel<W, OP_SHL><<<grid, 256, 0, st>>>(a); break;
+    case OP_SHR: vfb_compose_kernel<W, OP_SHR><<<grid, 256, 0, st>>>(a); break;
+    case OP_DIV: vfb_compose_kernel<W, OP_DIV><<<grid, 256, 0, st>>>(a); break;
+    default: vfb_compose_kernel<W, OP_MOD><<<grid, 256, 0, st>>>(a); break;
   }
 }
 
@@ -372,6 +470,13 @@ static int vfb_typed(const HostInstance& h, int max_len, const EngineOptions& o,
   a.keys = keys.as<unsigned long long>();
   a.vals = vals.as<unsigned>();
   a.mask = slots - 1;
+  a.shift = 64;
+  for (unsigned long long q = slots; q > 1; q >>= 1) --a.shift;
+  a.fp_mask = ~0ULL;
+  if (const char* fb = getenv("SIMBA_VFB_FP_BITS")) {
+    const int b = atoi(fb);
+    if (b >= 1 && b < 64) a.fp_mask = (1ULL << b) - 1;
+  }
   a.nrows = scal.as<unsigned long long>();
   a.cap = cap;
   a.target = tgt.as<W>();
@@ -421,6 +526,8 @@ static int vfb_typed(const HostInstance& h, int max_len, const EngineOptions& o,
                                                           tile_smem));
     tile_grid = sms * std::max(occ, 1);
   }
+  const bool ext = o.grammar == 1;  // the extended operators (ext_grammar.h)
+  const int nops = ext ? kExtOps : 8;
   int launch = 0;
   struct LaunchInfo {
     int op;
@@ -437,7 +544,8 @@ static int vfb_typed(const HostInstance& h, int max_len, const EngineOptions& o,
     }
     info.clear();
     const int first_launch = launch;
-    for (int op = 0; op < 8; ++op) {
+    for (int oi = 0; oi < nops; ++oi) {
+      const int op = ext ? ext_code(oi) : oi;
       if (is_unary(op)) {
         a.l0 = start[L - 1];
         a.nl = start[L] - start[L - 1];
@@ -455,13 +563,14 @@ static int vfb_typed(const HostInstance& h, int max_len, const EngineOptions& o,
           a.nl = start[i + 1] - start[i];
           a.r0 = start[j];
           a.nr = start[j + 1] - start[j];
-          a.swap = op == OP_SUB ? 1 : 0;
+          // non-commutative operators also compose the swapped pair
+          a.swap = (op == OP_SUB || op >= OP_SHL) ? 1 : 0;
           const unsigned long long n = (a.nl * a.nr) << a.swap;
           if (n == 0) continue;
           a.launch = launch++;
           info.push_back({op, n});
           const unsigned long long tiles = ((a.nl + kTL - 1) / kTL) * ((a.nr + kTR - 1) / kTR);
-          if (tiled)
+          if (tiled && op < OP_SHL)  // the extended operators: one pair per thread
             launch_tiled<W>(op, (int)std::min<unsigned long long>(tiles, tile_grid), tile_smem, st, a);
           else
             launch_compose<W>(op, (int)std::min<unsigned long long>((n + 255) / 256, grid), st, a);
@@ -475,6 +584,10 @@ static int vfb_typed(const HostInstance& h, int max_len, const EngineOptions& o,
     const int fl = (int)(hs[2] & 0xFFFFFFFFULL);
     const int full = (int)(hs[2] >> 32);
     const int hfull = (int)(hs[3] & 0xFFFFFFFFULL);
+    if (hs[3] >> 32) {
+      set_last_error("VFB hash slot not published within its wait limit");
+      return SIMBA_E_INTERNAL;
+    }
     const unsigned long long nrows = std::min<unsigned long long>(hs[0], cap);
     // reference-rule candidate count: every launch up to the one that found
     for (size_t q = 0; q < info.size(); ++q)
@@ -508,7 +621,7 @@ static int vfb_typed(const HostInstance& h, int max_len, const EngineOptions& o,
           if (cudaMemcpy(&r, rr.as<uint32_t>() + row, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
           if (build(rop, rl, rr, l, k, p, depth + 1)) return -1;
           if (!is_unary(op) && build(rop, rl, rr, r, k, p, depth + 1)) return -1;
-          p->push_back(op_char(op));
+          p->push_back(code_char(op));
           return 0;
         }
       };
@@ -519,7 +632,7 @@ static int vfb_typed(const HostInstance& h, int max_len, const EngineOptions& o,
         set_last_error("VFB expression reconstruction failed");
         return SIMBA_E_INTERNAL;
       }
-      post.push_back(op_char(out->op));
+      post.push_back(code_char(out->op));
       out->postfix = post;
       status = SIMBA_OK;
       break;
@@ -541,7 +654,7 @@ static int vfb_typed(const HostInstance& h, int max_len, const EngineOptions& o,
   // 12-byte hash probe, one written row per stored vector
   out->bytes_moved = (double)out->candidates * (2.0 * S * sizeof(W) + 12.0) +
                      (double)out->rows_total * S * sizeof(W);
-  if (status == SIMBA_OK && !host_check(out->postfix, h)) {
+  if (status == SIMBA_OK && !(ext ? ext_vector_check(out->postfix, h) : host_check(out->postfix, h))) {
     set_last_error("VFB answer failed the host re-check");
     return SIMBA_E_INTERNAL;
   }
@@ -554,6 +667,10 @@ int vfb_run(const HostInstance& h, int max_len, const EngineOptions& o, int inve
   if (rc) return rc;
   if (max_len < 1 || max_len > 100) {
     set_last_error("maxLen must be between 1 and 100");
+    return SIMBA_E_ARG;
+  }
+  if (o.grammar == 1 && (inverted || h.k > kExtMaxTerms)) {
+    set_last_error("the extended grammar takes at most 10 terminals and exact dedup");
     return SIMBA_E_ARG;
   }
   int ndev = 0;

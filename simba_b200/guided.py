@@ -219,3 +219,49 @@ def solve_guided(inst: Instance, max_size: int, prior: np.ndarray, **kw) -> Resu
     if pr.size != N_CLASSES:
         raise ValueError("prior must have 64 entries")
     return solve(inst, max_size, class_prior=pr, **kw)
+
+
+# ---------------------------------------------------------------------------
+# The proposal's training and evaluation workloads (seeded, synthetic).
+
+def training_set(n: int, seed0: int = 10 ** 6, max_size: int = 14, budget: float = 0.0,
+                 device: int = 0) -> Tuple[List[Instance], np.ndarray]:
+    """Instances for training the proposal: random targets of size 3-13 over
+    1-4 variables (+ the constant 1), 64 uint64 samples, seeds seed0.., solved
+    by the plain batch search and labelled with the shape class of the
+    answer (unsolved ones are dropped)."""
+    insts = list(iter_batch(n, seed0, sizes=range(3, 14), vars_=(1, 2, 3, 4), samples=(64,),
+                            word_bits=64))
+    return label_instances(insts, max_size, budget=budget, device=device)
+
+
+def mixed_batch(n: int, seed0: int = 5 * 10 ** 6) -> List[Instance]:
+    """The guided-and-batched workload: variables 2-5 (+ the constant 1),
+    target size 7-19, samples {32, 64, 128}, uint64 words."""
+    return list(iter_batch(n, seed0, sizes=range(7, 20), vars_=(2, 3, 4, 5),
+                           samples=(32, 64, 128), word_bits=64))
+
+
+def oracle_priors(results: Sequence[Result]) -> np.ndarray:
+    """The best prior any proposal could give: all mass on the shape class of
+    the answer the plain search found (uniform where it found none).  A guided
+    run with these priors bounds what guidance can gain on that batch."""
+    pri = np.full((len(results), N_CLASSES), 1.0 / N_CLASSES, dtype=np.float32)
+    for i, r in enumerate(results):
+        if r.status == OK:
+            pri[i] = 1e-6
+            pri[i, shape_class(r.postfix)] = 1.0
+    return pri
+
+
+def time_stats(results: Sequence[Result]) -> dict:
+    """Solved fraction and time-to-solution percentiles (device clock);
+    unsolved instances count as infinitely slow in the all-instance figures."""
+    solved = sorted(r.seconds for r in results if r.status == OK)
+    every = sorted([r.seconds if r.status == OK else float("inf") for r in results])
+
+    def pct(xs, q):
+        return xs[min(len(xs) - 1, int(q * len(xs)))] if xs else None
+    return {"solved_frac": len(solved) / max(1, len(results)),
+            "p50_s": pct(every, 0.5), "p95_s": pct(every, 0.95),
+            "p50_solved_s": pct(solved, 0.5), "p95_solved_s": pct(solved, 0.95)}

@@ -116,3 +116,18 @@ def test_rtid_option_is_rejected_where_unsupported():
                  lambda: S.solve(inst, 8, rtid=True, class_prior=prior)):
         with pytest.raises(S.SimbaError, match="rank_order|RTid"):
             call()
+
+
+def test_noalloc_rejects_options_it_does_not_run():
+    """The allocation-free entry point runs the plain spine search only: a
+    guided prior or the one-thread-per-rank engine is refused before any GPU
+    work instead of being silently dropped."""
+    import numpy as np
+    import simba_b200 as S
+    from simba_b200.instances import make_instance
+    inst = make_instance(5, 2, 16, 1, word_bits=64)
+    prior = np.ones(64, dtype=np.float32)
+    for call in (lambda: S.solve_noalloc(inst, 8, naive=True),
+                 lambda: S.solve_noalloc(inst, 8, class_prior=prior)):
+        with pytest.raises(S.SimbaError, match="plain spine search only"):
+            call()

@@ -261,3 +261,36 @@ def test_oracle_matches_widened_reference_u64(oracle):
         assert o["found"] and (len(p), OPS.index(p[-1])) == (o["size"], o["op"])
         same += p == o["postfix"]
     assert same >= 30
+
+
+def test_ext_grammar_oracle_bijection_and_semantics(oracle):
+    """Extended grammar oracle: unranking is a bijection of each size (every
+    rank gives a distinct postfix that parses back to a well-formed tree);
+    shifts by the word width or more give 0; division and modulo by zero
+    give the dividend per sample."""
+    t = oracle.ext_count_table(6, 3)
+    assert [int(t[s][12]) for s in range(1, 5)] == [3, 6, 102, 474]
+    for s in range(2, 6):
+        seen = {oracle.ext_unrank(r, s, t) for r in range(int(t[s][12]))}
+        assert len(seen) == int(t[s][12])
+    ev = oracle.ext_eval1
+    assert ev("01<", [5, 3], 64) == 40 and ev("01<", [5, 64], 64) == 0
+    assert ev("01<", [5, 31], 32) == (5 << 31) & 0xFFFFFFFF and ev("01<", [5, 32], 32) == 0
+    assert ev("01>", [2 ** 63, 63], 64) == 1 and ev("01>", [7, 70], 64) == 0
+    assert ev("01/", [7, 0], 64) == 7 and ev("01%", [7, 0], 64) == 7
+    assert ev("01/", [7, 2], 64) == 3 and ev("01%", [7, 2], 64) == 1
+
+
+def test_ext_vfb_oracle_whole_vector_division_rule(oracle):
+    """VFB composes whole vectors: a divisor vector with one zero element makes
+    v0 / v1 equal to v0 on every sample, so with that target VFB finds v0 at
+    size 1 while the target v0 / v1 evaluated per sample differs."""
+    import numpy as np
+    ins = np.array([[9, 0, 1], [8, 3, 1], [7, 2, 1]], dtype=np.uint64)
+    per_sample = np.array([oracle.ext_eval1("01/", r, 64) for r in ins], dtype=np.uint64)
+    assert list(per_sample) == [9, 2, 3]
+    o = oracle.ext_vfb(ins, per_sample, 4, 64)
+    # v0 / v1 as a whole vector is v0 (a zero divisor), so it is not the target
+    assert not (o["found"] and o["postfix"] == "01/")
+    p = oracle.ext_search(ins, per_sample, 4, 64)
+    assert p["found"] and p["size"] == 3 and p["postfix"] == "01/"

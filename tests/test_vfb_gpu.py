@@ -99,3 +99,23 @@ def test_vfb_cli_dropin(tmp_path, oracle, golden):
             assert len(infix_to_postfix(expr)) == len(infix_to_postfix(r["expr"]))
         else:
             assert expr == "Not found !"
+
+
+@pytest.mark.parametrize("fp_bits", [10, 16])
+def test_vfb_exact_dedup_under_forced_fingerprint_collisions(oracle, monkeypatch, fp_bits):
+    """With only `fp_bits` bits of the 64-bit fingerprint kept, thousands of
+    distinct vectors share a fingerprint; the exact dedup compares stored
+    rows element by element, so the rows per size (distinct vectors) still
+    equal the oracle's exact vector sets, unsatisfiable targets included."""
+    monkeypatch.setenv("SIMBA_VFB_FP_BITS", str(fp_bits))
+    for seed, bits in ((0, 64), (1, 32), (2, 64)):
+        inst = make_instance(7, 2, 32, 4000 + seed, word_bits=bits, unsat=seed == 2)
+        res = S.vfb_solve(inst, 7)
+        o = oracle.vfb(inst.inputs, inst.outputs, 7, bits)
+        assert res.found == o["found"]
+        last = res.size if res.found else 7
+        for L in range(1, last):
+            assert res.rows_per_size[L] == o["rows_per_size"][L], (fp_bits, seed, L, res, o)
+        if o["found"]:
+            assert res.size == o["size"] and res.op == o["op"]
+            assert oracle.check(res.postfix, inst.inputs, inst.outputs, bits)

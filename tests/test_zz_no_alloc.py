@@ -48,3 +48,22 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     inst = make_instance(15, 3, 64, 9, word_bits=64, unsat=True)
     with pytest.raises(S.SimbaError, match="static scratch"):
         S.solve_noalloc(inst, 20)
+
+
+def test_noalloc_allocates_no_device_memory():
+    """The promise itself: after a warm-up call of each case (which loads the
+    kernels and looks up the static array), repeated calls leave the free
+    device memory unchanged to the byte."""
+    import torch
+    insts = [make_instance(9, 2, 32, 0, word_bits=64), make_instance(10, 2, 16, 5, word_bits=32),
+             make_instance(12, 3, 64, 9, word_bits=64, unsat=True)]
+    for inst in insts:
+        S.solve_noalloc(inst, 12)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    for _ in range(3):
+        for inst in insts:
+            S.solve_noalloc(inst, 12)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0
