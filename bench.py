@@ -41,6 +41,8 @@ import threading
 import time
 from pathlib import Path
 
+import numpy as np
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
@@ -200,6 +202,48 @@ def pct(xs, q):
     return xs[min(len(xs) - 1, int(q * len(xs)))]
 
 
+def guided_batch(S, device: int) -> dict:
+    """Guided vs plain on the 16384-instance mixed batch (variables 2-5 + 1,
+    target size 7-19, samples {32,64,128}, uint64, max size 20, 60 s budget,
+    12 MiB of value tables per instance, device-clock times).  The proposal is
+    trained here by the project's kernels on instances the plain batch search
+    solved (size 3-13, 1-4 variables, seeds 10^6+).  A third run takes the
+    best prior any proposal could give -- all mass on the class of the plain
+    answer -- and bounds what guidance can gain on this batch."""
+    from simba_b200 import guided as G
+    t0 = time.perf_counter()
+    train, labels = G.training_set(20000, budget=30, device=device)
+    t_label = time.perf_counter() - t0
+    prop = G.Proposal(device=device, seed=0)
+    t0 = time.perf_counter()
+    losses = G.train(prop, train, labels, epochs=4, batch=256, lr=1e-3)
+    t_train = time.perf_counter() - t0
+    batch = G.mixed_batch(16384)
+    kw = dict(table_bytes=12 << 20, budget=60, device=device)
+    plain, st_p = S.solve_batch(batch, 20, **kw)
+    pri = prop.predict(batch)
+    guided, st_g = S.solve_batch(batch, 20, class_prior=pri, **kw)
+    ceil, st_c = S.solve_batch(batch, 20, class_prior=G.oracle_priors(plain), **kw)
+    prop.close()
+    both = [(p, g) for p, g in zip(plain, guided) if p.status == S.OK and g.status == S.OK]
+    labels_true = [G.shape_class(r.postfix) if r.status == S.OK else -1 for r in plain]
+    acc = float(np.mean([int(pr.argmax()) == c for pr, c in zip(pri, labels_true) if c >= 0]))
+    res = {"workload": "16384 instances: 2-5 vars + const 1, target size 7-19, samples {32,64,128}, "
+                       "uint64, max size 20, 60 s budget, 12 MiB tables per instance",
+           "proposal": {"train_instances": len(train), "label_s": t_label, "train_s": t_train,
+                        "final_loss": float(np.mean(losses[-20:])) if losses else None,
+                        "top1_on_batch": acc},
+           "plain": G.time_stats(plain), "guided": G.time_stats(guided),
+           "oracle_prior": G.time_stats(ceil),
+           "same_minimal_size": all(p.size == g.size for p, g in both),
+           "kernel_s": {"plain": st_p["kernel_ms"] / 1e3, "guided": st_g["kernel_ms"] / 1e3,
+                        "oracle_prior": st_c["kernel_ms"] / 1e3}}
+    for k in ("guided", "oracle_prior"):
+        a, b = res["plain"]["p50_s"], res[k]["p50_s"]
+        res[f"p50_ratio_plain_over_{k}"] = a / b if a and b and b != float("inf") else None
+    return res
+
+
 def secondary(a, S, sess, inst, device: int, stream) -> dict:
     """Measurements beside the headline, on one GPU, outside its timed
     region: the larger sizes 2..14 sweep (same instance, resident), the
@@ -234,11 +278,11 @@ def secondary(a, S, sess, inst, device: int, stream) -> dict:
 
     insts = list(iter_batch(4096, 0, sizes=range(5, 16), vars_=(1, 2, 3, 4),
                             samples=(16, 32, 64, 128), word_bits=64))
-    tuned = autotune.tune_batch(insts, device=device)
-    for i in insts:
-        i.unit_log2 = tuned[(i.num_variables, i.num_examples, i.word_bits)]
     t0 = time.perf_counter()
-    res, st = S.solve_batch(insts, 18, budget=60, device=device)
+    tuned, knobs = autotune.tune_batch_knobs(insts, device=device)  # sets each unit_log2
+    t_tune = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    res, st = S.solve_batch(insts, 18, budget=60, device=device, **knobs)
     wall = time.perf_counter() - t0
     solved = [r.seconds for r in res if r.status == S.OK]
     every = [r.seconds if r.status == S.OK else float("inf") for r in res]
@@ -249,12 +293,16 @@ def secondary(a, S, sess, inst, device: int, stream) -> dict:
         "p50_solved_s": pct(solved, 0.5), "p95_solved_s": pct(solved, 0.95),
         "candidate_evals_per_kernel_s": st["evaluated"] / max(st["kernel_ms"] / 1e3, 1e-9),
         "rounds": st["rounds"], "launches": st["launches"], "wall_s": wall,
-        "units": {f"k{k[0]}_S{k[1]}": v for k, v in sorted(tuned.items())}}
+        "autotune_s": t_tune, "batch_knobs": knobs,
+        "knobs": {f"k{k[0]}_S{k[1]}": v for k, v in sorted(tuned.items())}}
+
+    out["guided_16384"] = guided_batch(S, device)
 
     sat = make_instance(TARGET_SIZE, N_VARS, N_SAMPLES, 1, word_bits=64)
     v1 = S.vfb_solve(sat, 20, budget=60, device=device)
-    S.vfb_solve(inst, 9, device=device)  # warm-up
-    v2 = S.vfb_solve(inst, 11, budget=120, device=device)
+    rows = 40_000_000  # 20 GB of 512-byte vectors: room for every distinct vector to maxLen 11
+    S.vfb_solve(inst, 9, device=device, cache_rows=rows)  # warm-up
+    v2 = S.vfb_solve(inst, 11, budget=120, device=device, cache_rows=rows)
     peaks = {}
     try:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())

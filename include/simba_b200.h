@@ -93,6 +93,12 @@ typedef struct {
                             search the dividend per sample (x/0 = x%0 = x);
                             at most 10 terminals.  The plain search runs one
                             thread per rank in this grammar.               */
+  int32_t lanes_log2;    /* spine kernel layout: each group of contexts keeps at
+                            least 2^lanes_log2 of a CTA's 256 threads on its
+                            bottom values (0 = as many context groups as there
+                            are contexts); tuned by the Python autotuner      */
+  int32_t filter_samples;/* match filters: samples 1..filter_samples get value
+                            tables (1..3; 0 = 3)                               */
 } simba_options;
 
 typedef struct {

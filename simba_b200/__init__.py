@@ -44,7 +44,8 @@ class _Options(C.Structure):
                 ("table_bytes", C.c_int64), ("stream", C.c_uint64),
                 ("vfb_cache_rows", C.c_int64), ("vfb_reference_dedup", C.c_int32),
                 ("unit_log2", C.c_int32), ("class_prior", C.POINTER(C.c_float)),
-                ("rank_order", C.c_int32), ("grammar", C.c_int32)]
+                ("rank_order", C.c_int32), ("grammar", C.c_int32),
+                ("lanes_log2", C.c_int32), ("filter_samples", C.c_int32)]
 
 
 class _BatchResult(C.Structure):
@@ -181,7 +182,8 @@ class _Arrays:
 
 def _opts(device=0, complete=False, verbose=False, naive=False, budget=0.0,
           table_bytes=0, stream=0, cache_rows=0, reference_dedup=False,
-          unit_log2=0, class_prior=None, rtid=False, extended=False) -> _Options:
+          unit_log2=0, class_prior=None, rtid=False, extended=False, lanes_log2=0,
+          filter_samples=0) -> _Options:
     o = _Options()
     o.device = device
     o.size_range = 1 if complete else 0
@@ -195,6 +197,8 @@ def _opts(device=0, complete=False, verbose=False, naive=False, budget=0.0,
     o.unit_log2 = int(unit_log2)
     o.rank_order = 1 if rtid else 0
     o.grammar = 1 if extended else 0
+    o.lanes_log2 = int(lanes_log2)
+    o.filter_samples = int(filter_samples)
     if class_prior is not None:  # the caller keeps the array alive for the call
         o.class_prior = class_prior.ctypes.data_as(C.POINTER(C.c_float))
     return o

@@ -149,6 +149,8 @@ static EngineOptions to_opts(const simba_options* o) {
     e.class_prior = o->class_prior;
     e.rank_order = o->rank_order;
     e.grammar = o->grammar;
+    e.lanes_log2 = o->lanes_log2 < 0 ? 0 : o->lanes_log2;
+    e.filter_samples = o->filter_samples;
   }
   return e;
 }

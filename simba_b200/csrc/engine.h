@@ -34,6 +34,8 @@ struct EngineOptions {
   const float* class_prior = nullptr;  // guided search: 64 shape-class priors
   int rank_order = 0;        // 0 rank order, 1 RTid order (single-instance solve only)
   int grammar = 0;           // 0 the reference grammar, 1 extended (ext_grammar.h)
+  int lanes_log2 = 0;        // spine kernel: at least 2^lanes_log2 value lanes per context group
+  int filter_samples = 0;    // match-filter samples with value tables, 1..3 (0 = 3)
 };
 
 // Per-solve outcome filled by the engines (capi.cpp formats the strings).

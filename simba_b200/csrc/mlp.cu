@@ -10,8 +10,9 @@
 //             not exist).
 //   network   Z1 = X W1 + b1, H1 = relu(Z1), Z2 = H1 W2 + b2, H2 = relu(Z2),
 //             Z3 = H2 W3 + b3, p = softmax(Z3), loss = mean cross-entropy.
-//   GEMMs     BF16 operands, FP32 accumulation, tensor cores through
-//             mma.sync m16n8k16 (64x64 CTA tiles, four warps of 32x32).
+//   GEMMs     BF16 operands, FP32 accumulation, tcgen05.mma on the
+//             5th-generation tensor cores with the accumulator in TMEM
+//             (128x64 CTA tiles, gemm_tc_kernel).
 //   training  hand-written backward pass and Adam (FP32 master weights,
 //             BF16 copies feed the GEMMs).
 #include <cuda_bf16.h>
@@ -67,87 +68,160 @@ __global__ void features_kernel(const unsigned long long* in, const unsigned lon
 
 // ---------------------------------------------------------------- GEMM
 
-// C[M x N] = op(A)[M x K] * op(B)[K x N] (+ bias[n]), FP32 out.
-// op(A)(m,k) = TA ? A[k*lda + m] : A[m*lda + k]
-// op(B)(k,n) = TB ? B[n*ldb + k] : B[k*ldb + n]
-template <bool TA, bool TB>
-__global__ void __launch_bounds__(128) gemm_bf16_kernel(int M, int N, int K, const bf16* A, int lda,
-                                                        const bf16* B, int ldb, float* C, int ldc,
-                                                        const float* bias) {
-  constexpr int BM = 64, BN = 64, BK = 32, PAD = 8;
-  __shared__ __align__(16) bf16 As[BM][BK + PAD];  // m x k
-  __shared__ __align__(16) bf16 Bs[BN][BK + PAD];  // n x k
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int g = lane >> 2, t = lane & 3;
-  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  float acc[2][4][4];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.f;
-  const bf16 zero = __float2bfloat16(0.f);
-  for (int k0 = 0; k0 < K; k0 += BK) {
-    for (int e = tid; e < BM * BK; e += 128) {
-      const int mm = e / BK, kk = e % BK;
-      const int gm = m0 + mm, gk = k0 + kk;
-      bf16 va = zero;
-      if (gm < M && gk < K) va = TA ? A[(long long)gk * lda + gm] : A[(long long)gm * lda + gk];
-      As[mm][kk] = va;
-      const int gn = n0 + mm;
-      bf16 vb = zero;
-      if (gn < N && gk < K) vb = TB ? B[(long long)gn * ldb + gk] : B[(long long)gk * ldb + gn];
-      Bs[mm][kk] = vb;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int ks = 0; ks < BK; ks += 16) {
-      unsigned a[2][4], b[4][2];
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int r = wm + i * 16 + g;
-        a[i][0] = *reinterpret_cast<const unsigned*>(&As[r][ks + 2 * t]);
-        a[i][1] = *reinterpret_cast<const unsigned*>(&As[r + 8][ks + 2 * t]);
-        a[i][2] = *reinterpret_cast<const unsigned*>(&As[r][ks + 8 + 2 * t]);
-        a[i][3] = *reinterpret_cast<const unsigned*>(&As[r + 8][ks + 8 + 2 * t]);
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int c = wn + j * 8 + g;
-        b[j][0] = *reinterpret_cast<const unsigned*>(&Bs[c][ks + 2 * t]);
-        b[j][1] = *reinterpret_cast<const unsigned*>(&Bs[c][ks + 8 + 2 * t]);
-      }
-#pragma unroll
-      for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          asm volatile(
-              "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-              "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-              : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
-              : "r"(a[i][0]), "r"(a[i][1]), "r"(a[i][2]), "r"(a[i][3]), "r"(b[j][0]), "r"(b[j][1]));
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int row = m0 + wm + i * 16 + g + (r >= 2 ? 8 : 0);
-        const int col = n0 + wn + j * 8 + 2 * t + (r & 1);
-        if (row < M && col < N) C[(long long)row * ldc + col] = acc[i][j][r] + (bias ? bias[col] : 0.f);
-      }
+// C[M x N] = A[M x K] * Bt[N x K]^T (+ bias[n]) on the 5th-generation tensor
+// cores: tcgen05.mma (kind::f16, BF16 operands, FP32 accumulation in TMEM),
+// one elected thread issuing, the accumulator read back with tcgen05.ld.
+//   * One CTA (4 warps) per 128 x 64 tile of C; K in steps of 64.
+//   * Operands are staged in shared memory in the canonical K-major layout
+//     without swizzle: 8 x 8 core matrices of 128 contiguous bytes (8 rows of
+//     16 bytes), core matrix (row group i, k group j) at (8 i + j) * 128, so
+//     the leading (K) byte offset is 128 and the stride (M/N) byte offset is
+//     1024; each MMA covers K = 16, i.e. two k groups (+256 bytes).
+//   * tcgen05.commit arrives on an mbarrier when the MMAs of a step are done;
+//     every wait is bounded and reports through *err.
+// Both operands are K-major (row stride lda / ldb elements, multiples of 8,
+// 16-byte aligned rows); the caller transposes where needed.
+constexpr int kTcM = 128, kTcN = 64, kTcK = 64;
+constexpr size_t kTcSmem = 48 * 1024;  // 24 KB of tiles; 48 KB keeps <= 4 CTAs (256 TMEM columns) per SM
+
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);   // start address
+  d |= (uint64_t)(128 >> 4) << 16;          // leading (K) byte offset
+  d |= (uint64_t)(1024 >> 4) << 32;         // stride (M/N) byte offset
+  d |= 1ull << 46;                          // descriptor version of sm_100
+  return d;                                 // base offset 0, no swizzle
 }
 
-template <bool TA, bool TB>
-static void gemm(cudaStream_t st, int M, int N, int K, const bf16* A, int lda, const bf16* B, int ldb,
-                 float* C, int ldc, const float* bias) {
-  dim3 grid((N + 63) / 64, (M + 63) / 64);
-  gemm_bf16_kernel<TA, TB><<<grid, 128, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc, bias);
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t phase) {
+  for (int i = 0; i < (1 << 22); ++i) {
+    uint32_t done;
+    asm volatile("{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 "selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(mbar), "r"(phase) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// rows [r0, r0 + nrows) x k [k0, k0 + 64) of a K-major matrix into the canonical tile
+__device__ __forceinline__ void tc_stage(uint8_t* tile, const bf16* G, int ld, int r0, int nrows_total,
+                                         int rows, int k0, int K) {
+  for (int c = threadIdx.x; c < rows * 8; c += blockDim.x) {
+    const int row = c >> 3, kc = c & 7;
+    const int gr = r0 + row, gk = k0 + kc * 8;
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (gr < nrows_total) {
+      const bf16* src = G + (size_t)gr * ld + gk;
+      if (gk + 8 <= K) {
+        v = *reinterpret_cast<const uint4*>(src);
+      } else if (gk < K) {
+        __align__(16) bf16 e[8];
+        for (int q = 0; q < 8; ++q) e[q] = gk + q < K ? src[q] : __float2bfloat16(0.f);
+        v = *reinterpret_cast<const uint4*>(e);
+      }
+    }
+    *reinterpret_cast<uint4*>(tile + ((row >> 3) * 8 + kc) * 128 + (row & 7) * 16) = v;
+  }
+}
+
+__global__ void __launch_bounds__(128) gemm_tc_kernel(int M, int N, int K, const bf16* A, int lda,
+                                                      const bf16* Bt, int ldb, float* C, int ldc,
+                                                      const float* bias, int* err) {
+  extern __shared__ __align__(1024) uint8_t tc_smem[];
+  uint8_t* sA = tc_smem;
+  uint8_t* sB = tc_smem + kTcM * kTcK * 2;
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_base;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&mbar);
+  if (warp == 0) {
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&tmem_base);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" :: "r"(dst));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(mb));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tmem_base;
+  const int m0 = blockIdx.y * kTcM, n0 = blockIdx.x * kTcN;
+  // kind::f16 instruction descriptor: FP32 D, BF16 A and B, both K-major, N, M
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
+                         ((uint32_t)(kTcM >> 4) << 24);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int k0 = 0; k0 < K && ok; k0 += kTcK) {
+    tc_stage(sA, A, lda, m0, M, kTcM, k0, K);
+    tc_stage(sB, Bt, ldb, n0, N, kTcN, k0, K);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // st.shared -> tensor core
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint32_t a0 = (uint32_t)__cvta_generic_to_shared(sA);
+      const uint32_t b0 = (uint32_t)__cvta_generic_to_shared(sB);
+#pragma unroll
+      for (int kk = 0; kk < kTcK / 16; ++kk) {
+        const uint64_t ad = tc_desc(a0 + kk * 256), bd = tc_desc(b0 + kk * 256);
+        const uint32_t accumulate = (k0 > 0 || kk > 0) ? 1u : 0u;
+        asm volatile("{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                     :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(accumulate));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   :: "r"(mb) : "memory");
+    }
+    __syncwarp();
+    if (!tc_wait(mb, phase)) {  // the tiles stay in use until the MMAs are done
+      ok = false;
+      atomicOr(err, 1);
+    }
+    phase ^= 1;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    __syncthreads();
+  }
+  if (ok) {  // warp w owns TMEM lanes (rows) 32 w .. 32 w + 31
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll
+    for (int j0 = 0; j0 < kTcN; j0 += 16) {
+      uint32_t r[16];
+      const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)j0;
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                   : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                     "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                     "=r"(r[14]), "=r"(r[15])
+                   : "r"(ta));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < M) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int col = n0 + j0 + j;
+          if (col < N) C[(size_t)row * ldc + col] = __uint_as_float(r[j]) + (bias ? bias[col] : 0.f);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" :: "r"(tmem));
+}
+
+// out[c][r] = in[r][c] for a rows x cols BF16 matrix; out rows are ldo
+// elements (>= rows, the tail zero-filled).
+__global__ void transpose_bf16_kernel(const bf16* in, int rows, int cols, int ldi, bf16* out, int ldo) {
+  __shared__ bf16 t[32][33];
+  const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+    const int r = r0 + y, c = c0 + threadIdx.x;
+    t[y][threadIdx.x] = (r < rows && c < cols) ? in[(size_t)r * ldi + c] : __float2bfloat16(0.f);
+  }
+  __syncthreads();
+  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+    const int c = c0 + y, r = r0 + threadIdx.x;
+    if (c < cols && r < ldo) out[(size_t)c * ldo + r] = t[threadIdx.x][y];
+  }
 }
 
 // ---------------------------------------------------------------- elementwise
@@ -240,6 +314,34 @@ long long mlp_param_count() {
 class Mlp {
  public:
   explicit Mlp(int device) : dev_(device) {}
+
+  // C = op(A) op(B) (+ bias) through gemm_tc_kernel: op(A)(m,k) = TA ?
+  // A[k*lda + m] : A[m*lda + k], op(B)(k,n) = TB ? B[n*ldb + k] : B[k*ldb + n].
+  // The tensor-core kernel takes K-major operands, so an operand stored the
+  // other way is transposed into scratch first (rows padded to 8 elements,
+  // zero-filled).  Errors are kept in gemm_rc_ until the caller checks.
+  template <bool TA, bool TB>
+  void gemm(int M, int N, int K, const bf16* A, int lda, const bf16* B, int ldb, float* C, int ldc,
+            const float* bias) {
+    if (gemm_rc_) return;
+    const int Kp = (K + 7) / 8 * 8;
+    const dim3 tb(32, 8);
+    if (TA) {  // A is stored K x M: make it M x Kp
+      if ((gemm_rc_ = ta_.reserve((size_t)M * Kp * 2) == cudaSuccess ? 0 : SIMBA_E_NOMEM)) return;
+      transpose_bf16_kernel<<<dim3((M + 31) / 32, (Kp + 31) / 32), tb, 0, st_>>>(A, K, M, lda, ta_.as<bf16>(), Kp);
+      A = ta_.as<bf16>();
+      lda = Kp;
+    }
+    if (!TB) {  // B is stored K x N: make it N x Kp
+      if ((gemm_rc_ = tb_.reserve((size_t)N * Kp * 2) == cudaSuccess ? 0 : SIMBA_E_NOMEM)) return;
+      transpose_bf16_kernel<<<dim3((N + 31) / 32, (Kp + 31) / 32), tb, 0, st_>>>(B, K, N, ldb, tb_.as<bf16>(), Kp);
+      B = tb_.as<bf16>();
+      ldb = Kp;
+    }
+    gemm_tc_kernel<<<dim3((N + kTcN - 1) / kTcN, (M + kTcM - 1) / kTcM), 128, kTcSmem, st_>>>(
+        M, N, K, A, lda, B, ldb, C, ldc, bias, err_.as<int>());
+    if (cudaGetLastError() != cudaSuccess) gemm_rc_ = SIMBA_E_CUDA;
+  }
   ~Mlp() {
     if (st_) cudaStreamDestroy(st_);
   }
@@ -254,6 +356,9 @@ class Mlp {
     SB_CUDA(v_.reserve(P * 4));
     SB_CUDA(wb_.reserve(P * 2));
     SB_CUDA(loss_.reserve(16));
+    SB_CUDA(err_.reserve(16));
+    SB_CUDA(cudaMemsetAsync(err_.p, 0, 16, st_));
+    SB_CUDA(cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
     // He-uniform initialisation of the weights, zero biases
     std::vector<float> h(P, 0.f);
     std::mt19937_64 rng(seed);
@@ -328,11 +433,11 @@ class Mlp {
     const float* b2 = b1 + kSizes[1] + kSizes[2];
     const float* b3 = b2 + kSizes[3] + kSizes[4];
     const bf16* X = X_.as<bf16>();
-    gemm<false, false>(st_, B, kHid, kFeat, X, kFeat, W1, kHid, z1_.as<float>(), kHid, b1);
+    gemm<false, false>(B, kHid, kFeat, X, kFeat, W1, kHid, z1_.as<float>(), kHid, b1);
     relu_bf16_kernel<<<512, 256, 0, st_>>>(z1_.as<float>(), h1_.as<bf16>(), (long long)B * kHid);
-    gemm<false, false>(st_, B, kHid, kHid, h1_.as<bf16>(), kHid, W2, kHid, z2_.as<float>(), kHid, b2);
+    gemm<false, false>(B, kHid, kHid, h1_.as<bf16>(), kHid, W2, kHid, z2_.as<float>(), kHid, b2);
     relu_bf16_kernel<<<512, 256, 0, st_>>>(z2_.as<float>(), h2_.as<bf16>(), (long long)B * kHid);
-    gemm<false, false>(st_, B, kCls, kHid, h2_.as<bf16>(), kHid, W3, kCls, z3_.as<float>(), kCls, b3);
+    gemm<false, false>(B, kCls, kHid, h2_.as<bf16>(), kHid, W3, kCls, z3_.as<float>(), kCls, b3);
     SB_CUDA(cudaMemsetAsync(loss_.p, 0, 4, st_));
     int* lab = nullptr;
     if (labels_host) {
@@ -356,23 +461,37 @@ class Mlp {
       float* gW3 = gb2 + kSizes[3];
       float* gb3 = gW3 + kSizes[4];
       // layer 3
-      gemm<true, false>(st_, kHid, kCls, B, h2_.as<bf16>(), kHid, dz3_.as<bf16>(), kCls, gW3, kCls, nullptr);
+      gemm<true, false>(kHid, kCls, B, h2_.as<bf16>(), kHid, dz3_.as<bf16>(), kCls, gW3, kCls, nullptr);
       colsum_kernel<<<1, kCls, 0, st_>>>(dz3_.as<bf16>(), B, kCls, gb3);
-      gemm<false, true>(st_, B, kHid, kCls, dz3_.as<bf16>(), kCls, W3, kCls, dh_.as<float>(), kHid, nullptr);
+      gemm<false, true>(B, kHid, kCls, dz3_.as<bf16>(), kCls, W3, kCls, dh_.as<float>(), kHid, nullptr);
       relu_back_kernel<<<512, 256, 0, st_>>>(dh_.as<float>(), z2_.as<float>(), dz2_.as<bf16>(),
                                              (long long)B * kHid);
       // layer 2
-      gemm<true, false>(st_, kHid, kHid, B, h1_.as<bf16>(), kHid, dz2_.as<bf16>(), kHid, gW2, kHid, nullptr);
+      gemm<true, false>(kHid, kHid, B, h1_.as<bf16>(), kHid, dz2_.as<bf16>(), kHid, gW2, kHid, nullptr);
       colsum_kernel<<<(kHid + 255) / 256, 256, 0, st_>>>(dz2_.as<bf16>(), B, kHid, gb2);
-      gemm<false, true>(st_, B, kHid, kHid, dz2_.as<bf16>(), kHid, W2, kHid, dh_.as<float>(), kHid, nullptr);
+      gemm<false, true>(B, kHid, kHid, dz2_.as<bf16>(), kHid, W2, kHid, dh_.as<float>(), kHid, nullptr);
       relu_back_kernel<<<512, 256, 0, st_>>>(dh_.as<float>(), z1_.as<float>(), dz1_.as<bf16>(),
                                              (long long)B * kHid);
       // layer 1
-      gemm<true, false>(st_, kFeat, kHid, B, X, kFeat, dz1_.as<bf16>(), kHid, gW1, kHid, nullptr);
+      gemm<true, false>(kFeat, kHid, B, X, kFeat, dz1_.as<bf16>(), kHid, gW1, kHid, nullptr);
       colsum_kernel<<<(kHid + 255) / 256, 256, 0, st_>>>(dz1_.as<bf16>(), B, kHid, gb1);
       SB_CUDA(cudaGetLastError());
     }
     SB_CUDA(cudaStreamSynchronize(st_));
+    {
+      int e = 0;
+      SB_CUDA(cudaMemcpy(&e, err_.p, 4, cudaMemcpyDeviceToHost));
+      const int rc = gemm_rc_;
+      gemm_rc_ = 0;
+      if (rc) {
+        set_last_error("tensor-core GEMM launch failed");
+        return rc;
+      }
+      if (e) {
+        set_last_error("tensor-core GEMM: an MMA completion wait timed out");
+        return SIMBA_E_INTERNAL;
+      }
+    }
     if (loss_out) {
       float l = 0;
       SB_CUDA(cudaMemcpy(&l, loss_.p, 4, cudaMemcpyDeviceToHost));
@@ -440,6 +559,8 @@ class Mlp {
   int dev_;
   cudaStream_t st_ = nullptr;
   long long step_ = 0;
+  int gemm_rc_ = 0;
+  DevBuf ta_, tb_, err_;
   DevBuf w_, g_, m_, v_, wb_, loss_, fin_, fout_, finst_, X_, z1_, z2_, z3_, h1_, h2_, p_, lab_, dz3_, dh_,
       dz2_, dz1_;
 };

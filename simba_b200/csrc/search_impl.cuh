@@ -63,11 +63,18 @@ constexpr int kPreG = 131072;  // the same queue per CTA in global memory, when 
                                // (8-byte entries: context << 32 | bottom index)
 // Tuning knobs (compile-time): contexts per thread, minimum resident CTAs
 // per SM.
+#ifndef SIMBA_NESTED_PACK16
+#define SIMBA_NESTED_PACK16 1  // masked nested compares: two candidates per 32-bit prefilter word
+#endif
 #ifndef SIMBA_KR
 #define SIMBA_KR 8
 #endif
+// Resident CTAs per SM the spine kernel is compiled for: 3 caps it at 85
+// registers (80 used, a few hundred bytes of spills), the occupancy its work
+// units were tuned at; left to itself the compiler picked 48 registers and
+// spilled the nested compare loop's constraints.
 #ifndef SIMBA_MINB
-#define SIMBA_MINB 0
+#define SIMBA_MINB 3
 #endif
 #if SIMBA_MINB > 0
 #define SIMBA_SPINE_BOUNDS __launch_bounds__(256, SIMBA_MINB)
@@ -134,6 +141,17 @@ struct Ctx {
   unsigned c;       // context index inside that spine
 };
 static_assert(sizeof(Item) % 16 == 0, "Item must be 16-byte sized");
+
+// First bottom index of an item: a whole tabled size split into shape-class
+// ranges for the guided search keeps its range start in lv[0].coef (a
+// depth-0 item has no levels); every other item starts at 0.  The candidate
+// of bottom index v of a depth-0 item has rank base + v.
+SB_HD uint64_t item_voff(const Item& it) { return it.depth == 0 ? it.lv[0].coef : 0; }
+
+// Match-filter samples with value tables (options.filter_samples, 0 = all).
+inline int filter_samples(const EngineOptions& o) {
+  return o.filter_samples > 0 ? std::min(o.filter_samples, kExtra) : kExtra;
+}
 
 // Work units of a spine: groups of `cpu` context blocks x value blocks.
 SB_HD uint64_t item_units(const Item& it) {
@@ -653,8 +671,8 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
   }
 
   const W* V = d.tab[it.bottom];
-  const unsigned long long v0 = vblk * it.vb;
-  const unsigned long long v1 = umin64(v0 + it.vb, it.nv);
+  const unsigned long long v0 = item_voff(it) + vblk * it.vb;
+  const unsigned long long v1 = umin64(v0 + it.vb, item_voff(it) + it.nv);
   const unsigned long long q0 = v0 / VW, q1 = (v1 + VW - 1) / VW;
   const uint4* V4 = reinterpret_cast<const uint4*>(V);
 
@@ -674,22 +692,53 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
       XH.c[j] = (H)X.c[j];
     }
   }
+  // Masked compares without explicit levels: the low 16 bits of two bottom
+  // values share one 32-bit word (yp), each context's low 16 mask and key bits
+  // are doubled the same way, z = (yp & Mp) ^ Kp has a zero half exactly where
+  // a candidate's low 16 bits pass, and (z - 0x00010001) & ~z keeps bit 15 or
+  // 31 set iff a half is zero (the borrow of a zero half sets its top bit; a
+  // nonzero half never does, and borrows cannot cross from a nonzero low
+  // half).  One subtraction and two bitwise operations test two candidates.
+  constexpr bool PACK = SIMBA_NESTED_PACK16 && E == 0 && !FULL;
+  unsigned Mp[PACK ? kR : 1], Kp[PACK ? kR : 1];
+  if (PACK) {
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      const unsigned m16 = (unsigned)M[r] & 0xFFFFu, k16 = (unsigned)K[r] & 0xFFFFu;
+      Mp[r] = m16 | (m16 << 16);
+      Kp[r] = k16 | (k16 << 16);
+    }
+  }
   auto test = [&](const uint4& raw, unsigned long long q) {
     W xs[VW];
     memcpy(xs, &raw, 16);
     bool hit = false;
+    if (PACK) {
+      unsigned acc = 0;
 #pragma unroll
-    for (int e = 0; e < VW; ++e) {
+      for (int e = 0; e < VW; e += 2) {
+        const unsigned yp = __byte_perm((unsigned)xs[e], (unsigned)xs[e + 1], 0x5410);
 #pragma unroll
-      for (int r = 0; r < kR; ++r) {
-        H y = (H)xs[e];
-        if (E > 0) {
-          H wh[EE];
-#pragma unroll
-          for (int j = 0; j < EE; ++j) wh[j] = (H)WX[r][j];
-          y = eval_explicit<H, E>(XH, wh, y);
+        for (int r = 0; r < kR; ++r) {
+          const unsigned z = (yp & Mp[r]) ^ Kp[r];
+          acc |= (z - 0x00010001u) & ~z;
         }
-        hit |= FULL ? (y == (H)K[r]) : ((H)(y & (H)M[r]) == (H)K[r]);
+      }
+      hit = (acc & 0x80008000u) != 0;
+    } else {
+#pragma unroll
+      for (int e = 0; e < VW; ++e) {
+#pragma unroll
+        for (int r = 0; r < kR; ++r) {
+          H y = (H)xs[e];
+          if (E > 0) {
+            H wh[EE];
+#pragma unroll
+            for (int j = 0; j < EE; ++j) wh[j] = (H)WX[r][j];
+            y = eval_explicit<H, E>(XH, wh, y);
+          }
+          hit |= FULL ? (y == (H)K[r]) : ((H)(y & (H)M[r]) == (H)K[r]);
+        }
       }
     }
     if (!hit) return;
@@ -780,8 +829,8 @@ __device__ void process_unit_generic(const Params<W>& p, const InstDesc<W>& d, S
   const unsigned long long vblk = local - cblk * it.vblocks;
   const int L = it.L;
   const int g = threadIdx.x / L, lane = threadIdx.x % L;
-  const unsigned long long v0 = vblk * it.vb;
-  const unsigned long long v1 = umin64(v0 + it.vb, it.nv);
+  const unsigned long long v0 = item_voff(it) + vblk * it.vb;
+  const unsigned long long v1 = umin64(v0 + it.vb, item_voff(it) + it.nv);
   const W* V = d.tab[it.bottom];
   for (int r = 0; r < kR; ++r) {
     const unsigned long long c = cblk * it.cb + (unsigned long long)g * kR + r;
@@ -882,7 +931,8 @@ __device__ void process_unit_join(const Params<W>& p, const InstDesc<W>& d, Smem
   // 3. probe with every bottom value of the block
   constexpr int VW = 16 / sizeof(W);
   const W* V = d.tab[it.bottom];
-  const unsigned long long v0 = vblk * it.vb, v1 = umin64(v0 + it.vb, it.nv);
+  const unsigned long long v0 = item_voff(it) + vblk * it.vb;
+  const unsigned long long v1 = umin64(v0 + it.vb, item_voff(it) + it.nv);
   const uint4* V4 = reinterpret_cast<const uint4*>(V);
   auto probe = [&](const uint4& raw, unsigned long long q) {
     W xs[VW];
@@ -1111,7 +1161,7 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
         dispatch_unit<W>(p, d, sm, js, it, lb, s_in, s_out);
         if (threadIdx.x == 0) {
           const unsigned long long c0 = b * it.cb, c1 = umin64(c0 + it.cb, it.nctx);
-          const unsigned long long v0 = vblk * it.vb, v1 = umin64(v0 + it.vb, it.nv);
+          const unsigned long long v0 = vblk * it.vb, v1 = umin64(v0 + it.vb, it.nv);  // a count
           atomicAdd(p.evaluated, (c1 - c0) * (v1 - v0));
         }
         if (b + 1 < b1) {  // filter and verify this block's matches before the next one
@@ -1416,7 +1466,8 @@ static inline void finish_structure(Item& it, uint64_t mask) {
 
 // Thread layout and work units: G groups of kR contexts x L lanes over the
 // bottom values, about 2^22 candidates per unit.
-static inline void finish_layout(Item& it, int threads, uint64_t unit_target = 1ULL << 22) {
+static inline void finish_layout(Item& it, int threads, uint64_t unit_target = 1ULL << 22,
+                                 int min_lanes = 1) {
   const uint64_t nctx = it.nctx;
   if (it.joinable && nctx >= kJoinMin) {  // hash join (full = 2)
     it.full = 2;
@@ -1432,7 +1483,10 @@ static inline void finish_layout(Item& it, int threads, uint64_t unit_target = 1
   }
   uint64_t groups = (nctx + kR - 1) / kR;
   int G = 1;
-  while (G < threads && (uint64_t)G < groups) G <<= 1;
+  // context groups double while they have contexts to take and each keeps
+  // at least min_lanes value lanes (the autotuned split of a CTA's threads
+  // between contexts and bottom values)
+  while (G < threads && (uint64_t)G < groups && threads / (G << 1) >= min_lanes) G <<= 1;
   it.G = (uint16_t)G;
   it.L = (uint16_t)(threads / G);
   it.cb = (uint32_t)(G * kR);
@@ -1495,6 +1549,44 @@ static inline void spine_classes(const Item& it, int size, int* c0, int* c1) {
   *c0 = L.op * 8 + std::min(left, 7);
 }
 
+// Guided search of a tabled size: the size's rank range (= its value table)
+// split into the contiguous ranges of its shape classes -- each operator
+// block, and inside a binary block each left size f (N(f) N(s-1-f) ranks,
+// class 8 op + min(f, 7)) -- as depth-0 items with their class prior, so that
+// the likely classes' ranges are searched first.  A unary block is one range
+// whose prior is its best unary-chain class.
+static inline void tabled_class_items(const CountTable& ct, int s, const float* prior,
+                                      std::vector<Item>* items) {
+  auto add = [&](uint64_t a, uint64_t n, float prio) {
+    if (n == 0) return;
+    Item it;
+    memset(&it, 0, sizeof(it));
+    it.depth = 0;
+    it.bottom = (int8_t)s;
+    it.coefv = 1;
+    it.nv = n;
+    it.lv[0].coef = a;  // item_voff
+    it.prio = prio;
+    items->push_back(it);
+  };
+  uint64_t off = 0;
+  for (int op = 0; op < 8; ++op) {
+    if (is_unary(op)) {
+      float p = 0.f;
+      for (int m = 1; m < 8; ++m) p = std::max({p, prior[OP_NOT * 8 + m], prior[OP_NEG * 8 + m]});
+      add(off, ct.n[s][op], p);
+      off += ct.n[s][op];
+      continue;
+    }
+    const int fmax = is_commutative(op) ? (s - 1) / 2 : s - 2;
+    for (int f = 1; f <= fmax; ++f) {
+      const uint64_t n = ct.n[f][8] * ct.n[s - 1 - f][8];
+      add(off, n, prior[op * 8 + std::min(f, 7)]);
+      off += n;
+    }
+  }
+}
+
 static inline float spine_prio(const Item& it, int size, const float* prior) {
   int a, b;
   spine_classes(it, size, &a, &b);
@@ -1516,7 +1608,9 @@ static inline void fuse_small(std::vector<Item>& items, std::vector<Item>* small
   std::vector<std::vector<size_t>> members;
   uint64_t total = 0;
   for (auto& it : items) {
-    const bool fusable = it.nexp == 0 && it.nctx < (uint64_t)kThreads * kR && total + it.nctx <= max_ctxs;
+    // a class range of a tabled size covers part of its bottom table: not fused
+    const bool fusable = it.nexp == 0 && it.nctx < (uint64_t)kThreads * kR && total + it.nctx <= max_ctxs &&
+                         item_voff(it) == 0 && it.nv == ct.n[(int)it.bottom][8];
     if (!fusable) {
       keep.push_back(it);
       continue;
@@ -1702,7 +1796,7 @@ class Search final : public SearchSession {
   // V_t on sample j (j = 0, and the filter samples 1..kExtra that exist): one
   // allocation per size t holds the tables of all samples
   W* tab(int t, int j = 0) const { return d_tabs_[t].as<W>() + (size_t)j * padded(ct_.n[t][8]); }
-  int nsamp() const { return std::min(h_.S, kExtra + 1); }
+  int nsamp() const { return std::min(h_.S, filter_samples(o_) + 1); }
 
   // Build V_{built+1} .. V_t (each entry one operator over smaller tables).
   int ensure_tables(int t) {
@@ -1800,7 +1894,9 @@ class Search final : public SearchSession {
     bool use_naive = !spine_ok || (s > T && (s - 1) / 2 > T);
     std::vector<Item> items;
     if (!use_naive) {
-      if (s <= T) {
+      if (s <= T && o_.class_prior && s >= 2) {
+        tabled_class_items(ct_, s, o_.class_prior, &items);
+      } else if (s <= T) {
         Item it;
         memset(&it, 0, sizeof(it));
         it.depth = 0;
@@ -1831,13 +1927,14 @@ class Search final : public SearchSession {
         finish_structure(it, mask_);
       }
       const bool guided = o_.class_prior != nullptr;
-      if (guided)
-        for (auto& it : items) it.prio = spine_prio(it, s, o_.class_prior);
+      if (guided)  // class ranges of a tabled size carry their prior already
+        for (auto& it : items)
+          if (it.depth > 0) it.prio = spine_prio(it, s, o_.class_prior);
       std::vector<Item> small;
       uint64_t nctxs = 0;
       fuse_small(items, &small, &nctxs, ct_, 1ULL << 22, guided);
       const uint64_t unit_target = 1ULL << (o_.unit_log2 > 0 ? std::min(o_.unit_log2, 40) : 22);
-      for (auto& it : items) finish_layout(it, kThreads, unit_target);
+      for (auto& it : items) finish_layout(it, kThreads, unit_target, 1 << std::min(o_.lanes_log2, 8));
       if (guided)  // most likely shape classes first; ties in rank order
         std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) {
           return a.prio != b.prio ? a.prio > b.prio : a.base < b.base;
@@ -2171,7 +2268,7 @@ class Batch {
     std::vector<int> nsamp(n);
     for (int i = 0; i < n; ++i) {
       const CountTable& ct = cts_[ct_of[i]];
-      nsamp[i] = std::min(hs_[i].S, kExtra + 1);  // sample-0 tables and the filter samples'
+      nsamp[i] = std::min(hs_[i].S, filter_samples(o_) + 1);  // sample-0 tables and the filter samples'
       const uint64_t ns = (uint64_t)nsamp[i];
       uint64_t tot = 0;  // every tabled size has the tables of all samples
       T[i] = 0;
@@ -2664,7 +2761,7 @@ class Batch {
       if (guided)  // fused groups stay inside one bucket
         for (auto& it : items) it.prio = (float)bucket_of(it, s);
       fuse_small(items, &tp.small, &tp.nctxs, ct, 1ULL << 22, guided);
-      for (auto& it : items) finish_layout(it, kThreads, unit_target);
+      for (auto& it : items) finish_layout(it, kThreads, unit_target, 1 << std::min(o_.lanes_log2, 8));
       // Spines of one kernel variant (fused / full compare / explicit
       // levels) run together: CTAs of a round work through a few lists at a
       // time, and mixing variants there thrashes the instruction cache.

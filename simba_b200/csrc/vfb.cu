@@ -206,6 +206,7 @@ __device__ int hash_claim_exact(const VfbArgs<W>& a, unsigned long long A, Elem 
 template <class W, int OP, class Elem>
 __device__ __forceinline__ void vfb_offer(const VfbArgs<W>& a, unsigned long long x, unsigned long long y,
                                           unsigned long long A, unsigned B, Elem elem) {
+  if (*(volatile int*)&a.flags[0]) return;  // the cache is full: nothing more is stored
   A &= a.fp_mask;
   unsigned long long slot = ~0ULL;
   if (a.inverted) {
@@ -250,6 +251,8 @@ __global__ void __launch_bounds__(256) vfb_compose_kernel(VfbArgs<W> a) {
   const int S = a.S;
   for (unsigned long long idx = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
        idx += (unsigned long long)gridDim.x * blockDim.x) {
+    // the cache or the hash table is full: the search ends with this size
+    if (*(volatile int*)&a.flags[0] | *(volatile int*)&a.flags[1]) break;
     const unsigned long long pair = a.swap ? idx >> 1 : idx;
     unsigned long long x, y;
     if (unary) {
@@ -296,11 +299,16 @@ __global__ void __launch_bounds__(256) vfb_tile_kernel(VfbArgs<W> a) {
   W* sr = sl + kTL * P;
   const unsigned long long tl = (a.nl + kTL - 1) / kTL, tr = (a.nr + kTR - 1) / kTR;
   const int ri = threadIdx.x % kTR, li0 = threadIdx.x / kTR;
+  __shared__ int s_stop;
   for (unsigned long long tile = blockIdx.x; tile < tl * tr; tile += gridDim.x) {
     const unsigned long long lb = (tile / tr) * kTL, rb = (tile % tr) * kTR;
     const int nl = (int)(a.nl - lb < (unsigned long long)kTL ? a.nl - lb : kTL);
     const int nr = (int)(a.nr - rb < (unsigned long long)kTR ? a.nr - rb : kTR);
+    // one read per CTA, so that every thread leaves the loop together: a full
+    // cache or hash table ends the search with this size
+    if (threadIdx.x == 0) s_stop = *(volatile int*)&a.flags[0] | *(volatile int*)&a.flags[1];
     __syncthreads();  // the previous tile's reads are done
+    if (s_stop) break;
     const W* gl = a.rows + (a.l0 + lb) * S;
     const W* gr = a.rows + (a.r0 + rb) * S;
     for (int q = threadIdx.x; q < nl * S; q += blockDim.x) sl[(q / S) * P + q % S] = gl[q];

@@ -260,8 +260,82 @@ def time_stats(results: Sequence[Result]) -> dict:
     solved = sorted(r.seconds for r in results if r.status == OK)
     every = sorted([r.seconds if r.status == OK else float("inf") for r in results])
 
-    def pct(xs, q):
-        return xs[min(len(xs) - 1, int(q * len(xs)))] if xs else None
+    def pct(xs, q):  # None where the percentile instance is unsolved
+        if not xs:
+            return None
+        v = xs[min(len(xs) - 1, int(q * len(xs)))]
+        return None if v == float("inf") else v
     return {"solved_frac": len(solved) / max(1, len(results)),
             "p50_s": pct(every, 0.5), "p95_s": pct(every, 0.95),
             "p50_solved_s": pct(solved, 0.5), "p95_solved_s": pct(solved, 0.95)}
+
+
+def heldout_set(n: int = 1024, seed0: int = 3 * 10 ** 6) -> List[Instance]:
+    """Held-out evaluation targets: random size 11-17 over 1-4 variables (+ the
+    constant 1), 64 uint64 samples (seeds disjoint from the training set's)."""
+    return list(iter_batch(n, seed0, sizes=range(11, 18), vars_=(1, 2, 3, 4), samples=(64,),
+                           word_bits=64))
+
+
+def label_in_chunks(insts: Sequence[Instance], max_size: int, chunk: int, budget: float,
+                    device: int = 0) -> Tuple[List[Instance], np.ndarray]:
+    """label_instances over consecutive chunks, each under its own budget."""
+    keep: List[Instance] = []
+    labels: List[int] = []
+    for s in range(0, len(insts), chunk):
+        k, l = label_instances(insts[s:s + chunk], max_size, budget=budget, device=device)
+        keep += k
+        labels += list(l)
+    return keep, np.asarray(labels, dtype=np.int32)
+
+
+def proposal_experiment(n_train: int = 200_000, n_eval: int = 1024, epochs: int = 4,
+                        label_chunk: int = 16384, label_budget: float = 30.0,
+                        eval_budget: float = 60.0, device: int = 0, seed: int = 0) -> dict:
+    """The learned-proposal experiment: train on `n_train` instances solved by
+    the plain batch search (training_set's distribution, max size 14), then
+    search the held-out targets (max size 20) plain, guided by the trained
+    proposal, and guided by the best possible prior (the plain answers'
+    classes), each as one batch under `eval_budget` seconds.  Returns the
+    timings, solved fractions, time-to-solution percentiles and the
+    proposal's top-1 accuracy on the held-out answers."""
+    import time
+    t0 = time.perf_counter()
+    train_insts = list(iter_batch(n_train, 10 ** 6, sizes=range(3, 14), vars_=(1, 2, 3, 4),
+                                  samples=(64,), word_bits=64))
+    keep, labels = label_in_chunks(train_insts, 14, label_chunk, label_budget, device)
+    t_label = time.perf_counter() - t0
+    prop = Proposal(device=device, seed=seed)
+    t0 = time.perf_counter()
+    losses = train(prop, keep, labels, epochs=epochs, batch=256, lr=1e-3, seed=seed)
+    t_train = time.perf_counter() - t0
+    ev = heldout_set(n_eval)
+    plain, st_p = solve_batch(ev, 20, budget=eval_budget, device=device)
+    pri = prop.predict(ev)
+    guided, st_g = solve_batch(ev, 20, budget=eval_budget, device=device, class_prior=pri)
+    best, st_b = solve_batch(ev, 20, budget=eval_budget, device=device,
+                             class_prior=oracle_priors(plain))
+    prop.close()
+    cls = [shape_class(r.postfix) if r.status == OK else -1 for r in plain]
+    top1 = [int(p.argmax()) == c for p, c in zip(pri, cls) if c >= 0]
+    both = [(a, b) for a, b in zip(plain, guided) if a.status == OK and b.status == OK]
+    out = {"train": {"instances": n_train, "labelled": len(keep), "label_s": t_label,
+                     "train_s": t_train, "epochs": epochs,
+                     "final_loss": float(np.mean(losses[-50:])) if losses else None},
+           "eval": {"instances": n_eval, "top1": float(np.mean(top1)) if top1 else None,
+                    "plain": time_stats(plain), "guided": time_stats(guided),
+                    "oracle_prior": time_stats(best),
+                    "same_minimal_size": all(a.size == b.size for a, b in both),
+                    "kernel_s": {"plain": st_p["kernel_ms"] / 1e3, "guided": st_g["kernel_ms"] / 1e3,
+                                 "oracle_prior": st_b["kernel_ms"] / 1e3}}}
+    for k in ("guided", "oracle_prior"):
+        a, b = out["eval"]["plain"]["p50_s"], out["eval"][k]["p50_s"]
+        out["eval"][f"p50_ratio_plain_over_{k}"] = a / b if a and b else None
+    return out
+
+
+if __name__ == "__main__":  # python -m simba_b200.guided [n_train] > result.json
+    import json
+    import sys
+    n = int(sys.argv[1]) if len(sys.argv) > 1 else 200_000
+    print(json.dumps(proposal_experiment(n_train=n), indent=1))

@@ -69,6 +69,28 @@ def test_autotuner_picks_a_candidate_and_caches(tmp_path, monkeypatch):
         assert (r.status, r.rank) == (one.status, one.rank)
 
 
+def test_autotuned_knobs_keep_answers(tmp_path, monkeypatch):
+    """All three tuned knobs (unit size, lanes per context group, filter
+    samples) are chosen from their candidate sets, and searches run with any
+    of them return the same answers as the defaults."""
+    from simba_b200 import autotune as A
+    monkeypatch.setenv("SIMBA_CACHE", str(tmp_path))
+    A._mem.clear()
+    k = A.tune_bucket_knobs(4, 64, 64)
+    assert k["unit_log2"] in A.CANDIDATES and k["lanes_log2"] in A.LANES
+    assert k["filter_samples"] in A.FILTERS
+    insts = list(iter_batch(24, 9100, sizes=range(5, 11), vars_=(3,), samples=(64,), word_bits=64))
+    base = [S.solve(i, 11) for i in insts]
+    for lanes, filt in ((0, 1), (2, 3), (4, 2)):
+        for inst, b in zip(insts, base):
+            r = S.solve(inst, 11, lanes_log2=lanes, filter_samples=filt, table_bytes=1 << 24)
+            assert (r.status, r.size, r.rank, r.postfix) == (b.status, b.size, b.rank, b.postfix)
+    per, opts = A.tune_batch_knobs(insts)
+    res, _ = S.solve_batch(insts, 11, **opts)
+    for r, b in zip(res, base):
+        assert (r.status, r.rank) == (b.status, b.rank)
+
+
 def test_guided_batch_finds_minimal_sizes(oracle):
     """Guided batch with per-instance priors: same minimal size as the plain
     batch, every answer verified, in one launch per size round."""
