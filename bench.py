@@ -62,14 +62,14 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the secondary objects (larger sweep, batch, VFB)")
-    ap.add_argument("--case", choices=["spine12", "sweep13", "batch10", "vfb10"],
+    ap.add_argument("--case", choices=["spine12", "spine13", "sweep13", "batch10", "vfb10"],
                     help="run one small profiling case instead of the benchmark (no JSON line)")
     return ap.parse_args()
 
 
 def run_case(name: str) -> None:
-    """Small cases for ncu captures (see profiles/): a size-12 sweep of the
-    benchmark instance run twice; the sizes 2..13 sweep run twice (the
+    """Small cases for ncu captures (see profiles/): a size-12 (size-13) sweep
+    of the benchmark instance run twice; the sizes 2..13 sweep run twice (the
     launch list of one benchmark step); a 256-instance mixed batch to max size 11
     (its 9th spine launch is the size-10 round); VFB to maxLen 10 on the
     benchmark instance."""
@@ -82,6 +82,11 @@ def run_case(name: str) -> None:
             for _ in range(2):
                 r = ss.sweep(12, 12)
         print("spine12", r.candidates, r.evaluated, r.kernel_ms)
+    elif name == "spine13":
+        with S.Session(inst) as ss:
+            for _ in range(2):
+                r = ss.sweep(13, 13)
+        print("spine13", r.candidates, r.evaluated, r.kernel_ms, r.join_ms, r.nested_ms)
     elif name == "sweep13":
         with S.Session(inst, verbose=True) as ss:
             for _ in range(2):
@@ -193,6 +198,53 @@ def cpu_baseline(inst, size: int) -> dict:
     return {"value": ev / dt, "unit": "candidate-evals/s", "cores": cores, "kind": "port",
             "sample": f"first {ev} ranks of size {size}, {N_SAMPLES} uint64 samples, "
                       f"{N_VARS} vars + const 1, unsatisfiable target ({dt:.1f} s)"}
+
+
+def roofline(kinds: dict, alg_ops: float, steps: int, int_peak: float, alu_peak: float) -> dict:
+    """Roofline of the search kernel per launch kind, per step.
+
+    The spine kernel runs two launches per size.  Nested compares (spines
+    with & or |) decide each candidate with a masked 64-bit compare, 3
+    algorithmic 32-bit lane operations (two AND-XOR halves and their
+    combination), all on the ALU pipe: achieved = those lane operations /
+    the launch time, against the ALU pipe's measured peak (simba_alu_peak).
+    Hash-join launches (the other spines) read each bottom value once per
+    block of contexts: achieved = the bottom tables' bytes, each counted once
+    per size (the algorithmic minimum) / the launch time, against the
+    measured HBM copy bandwidth; `streamed` is what the blocking actually
+    reads.  The dominant kind by time is the headline entry."""
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        pass
+    hbm = peaks.get("hbm_gbs")
+    hbm_src = "MEASURED_PEAKS.json hbm_gbs" if hbm else "fallback 6650 GB/s"
+    hbm = hbm or 6650.0
+    jm, nm = kinds["join_ms"] / steps, kinds["nested_ms"] / steps
+    join_alg = 5.0 * kinds["join_bytes_streamed"] / 8.0  # hash + filter test per value read
+    nested_ops = max(0.0, alg_ops - join_alg) / steps
+    nested = {"bound": "int-alu", "unit": "Tlane-ops/s", "kernel_ms": nm,
+              "candidates": kinds["nested_candidates"] / steps,
+              "achieved": nested_ops / (nm / 1e3) / 1e12 if nm > 0 else None,
+              "peak": alu_peak / 1e12, "peak_source": "measured live: simba_alu_peak (LOP3 chains)",
+              "alg_ops_per_candidate": nested_ops / max(1.0, kinds["nested_candidates"] / steps),
+              "traffic": None}
+    nested["frac"] = nested["achieved"] / nested["peak"] if nested["achieved"] else None
+    nested["frac_of_int_peak"] = (nested["achieved"] * 1e12 / int_peak) if nested["achieved"] else None
+    tb, sb = kinds["join_table_bytes"] / steps, kinds["join_bytes_streamed"] / steps
+    join = {"bound": "hbm", "unit": "GB/s", "kernel_ms": jm,
+            "candidates": kinds["join_candidates"] / steps,
+            "achieved": tb / (jm / 1e3) / 1e9 if jm > 0 else None, "peak": hbm,
+            "peak_source": hbm_src, "alg_bytes": tb, "streamed_bytes": sb,
+            "streamed_gbs": sb / (jm / 1e3) / 1e9 if jm > 0 else None, "traffic": None}
+    join["frac"] = join["achieved"] / hbm if join["achieved"] else None
+    head = dict(nested if nm >= jm else join)
+    head["kernel"] = "spine_kernel (" + ("nested-compare" if nm >= jm else "hash-join") + " launches)"
+    head["launch_kinds"] = {"nested": nested, "join": join}
+    head["note"] = ("traffic: DRAM bytes need an ncu capture, see profiles/; candidate-evals "
+                    "count candidates decided, by compare or by join probe")
+    return head
 
 
 def pct(xs, q):
@@ -351,12 +403,16 @@ def run_ours(a, rank: int, world: int, local_rank: int) -> None:
         torch.cuda.synchronize()
         e0.record(stream)
         kernel_ms, alg_ops, launches, evaluated = 0.0, 0, 0, 0
+        kinds = {"join_ms": 0.0, "nested_ms": 0.0, "join_candidates": 0, "nested_candidates": 0,
+                 "join_bytes_streamed": 0.0, "join_table_bytes": 0.0}
         for _ in range(a.steps):
             r = sess.sweep(2, L)
             kernel_ms += r.kernel_ms
             alg_ops += r.alg_ops
             launches += r.launches
             evaluated += r.evaluated
+            for k in kinds:
+                kinds[k] += getattr(r, k)
         e1.record(stream)
         torch.cuda.synchronize()
         clk = clocks.stop()
@@ -395,10 +451,7 @@ def run_ours(a, rank: int, world: int, local_rank: int) -> None:
     if rank == 0:
         peak = S.int_peak(local_rank)
         alu_peak = S.alu_peak(local_rank)
-        kernel_s = kernel_ms / 1e3
-        achieved = alg_ops / kernel_s if kernel_s > 0 else 0.0
-        # DRAM traffic needs an ncu capture (profiles/); a live run cannot count it
-        traffic = None
+        rl = roofline(kinds, alg_ops, a.steps, peak, alu_peak)
         out = {
             "metric": "candidate-evals/s", "value": value, "unit": "candidate-evals/s",
             "n_gpus": world, "steps": a.steps, "warmup": max(a.warmup, 3),
@@ -414,14 +467,7 @@ def run_ours(a, rank: int, world: int, local_rank: int) -> None:
                        "l2": "inputs larger than L2 (sample-0 value tables of sizes <= 10: 1.46 GB)",
                        "parallelism": f"independent instances x{world}"},
             "e2e": e2e,
-            "roofline": {"bound": "int-alu", "achieved": achieved / 1e12, "peak": peak / 1e12,
-                         "unit": "Tlane-ops/s", "frac": achieved / peak if peak else None,
-                         "traffic": traffic,
-                         "kernel": "spine_kernel", "kernel_ms_per_step": kernel_ms / a.steps,
-                         "alg_ops_per_candidate": alg_ops / max(1, evaluated),
-                         "peak_source": "measured live: simba_int_peak (LOP3+IMAD chains)",
-                         "alu_pipe_peak": alu_peak / 1e12,
-                         "frac_of_alu_pipe": achieved / alu_peak if alu_peak else None},
+            "roofline": rl,
             "gpu_launches": launches,
             "clocks": clk,
         }

@@ -943,7 +943,9 @@ int orc_ext_vfb(int bits, int k, int S, const uint64_t *in, const uint64_t *out,
         continue;
       }
       const int swap = !ext_comm(e);
-      for (int i = 1; 2 * i <= L - 1; ++i) {
+      /* the reference stops after the chunk (here: the split) that produced
+       * the target (generateMBAs, full-cache.cu:636-640) */
+      for (int i = 1; 2 * i <= L - 1 && st.found_row < 0; ++i) {
         const int j = L - 1 - i;
         for (int64_t x = start[i]; x < start[i + 1]; ++x) {
           for (int64_t y = start[j]; y < start[j + 1]; ++y) {

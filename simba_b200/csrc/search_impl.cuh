@@ -699,21 +699,31 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
   // 31 set iff a half is zero (the borrow of a zero half sets its top bit; a
   // nonzero half never does, and borrows cannot cross from a nonzero low
   // half).  One subtraction and two bitwise operations test two candidates.
+  // A 16-bit window passes a random value with probability 2^-(mask bits in
+  // it), so the packed test only pays where every context of the warp keeps
+  // at least kPackMinBits low mask bits; other warps (sparse masks, e.g. an &
+  // with a small value that has few bits set) take the 32-bit test, whose
+  // survivors are rarer.  The choice is uniform across the warp.
   constexpr bool PACK = SIMBA_NESTED_PACK16 && E == 0 && !FULL;
+  constexpr int kPackMinBits = 10;
   unsigned Mp[PACK ? kR : 1], Kp[PACK ? kR : 1];
+  bool use_pack = false;
   if (PACK) {
+    bool dense = true;
 #pragma unroll
     for (int r = 0; r < kR; ++r) {
       const unsigned m16 = (unsigned)M[r] & 0xFFFFu, k16 = (unsigned)K[r] & 0xFFFFu;
       Mp[r] = m16 | (m16 << 16);
       Kp[r] = k16 | (k16 << 16);
+      dense &= __popc(m16) >= kPackMinBits;
     }
+    use_pack = __all_sync(0xFFFFFFFFu, dense);
   }
   auto test = [&](const uint4& raw, unsigned long long q) {
     W xs[VW];
     memcpy(xs, &raw, 16);
     bool hit = false;
-    if (PACK) {
+    if (PACK && use_pack) {
       unsigned acc = 0;
 #pragma unroll
       for (int e = 0; e < VW; e += 2) {

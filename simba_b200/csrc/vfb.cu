@@ -193,7 +193,19 @@ __device__ int hash_claim_exact(const VfbArgs<W>& a, unsigned long long A, Elem 
     __threadfence();                  // the row's words were written before the publication
     const W* row = a.rows + (unsigned long long)(v - 1) * a.S;
     bool same = true;
-    for (int i = 0; i < a.S && same; ++i) same = load_cg<W>(row + i) == elem(i);
+    if ((a.S * sizeof(W)) % 16 == 0) {  // rows 16-byte aligned: 16-byte loads
+      constexpr int VW = 16 / sizeof(W);
+      const uint4* r4 = reinterpret_cast<const uint4*>(row);
+      for (int i = 0; i < a.S && same; i += VW) {
+        const uint4 q = __ldcg(r4 + i / VW);
+        W w[VW];
+        memcpy(w, &q, 16);
+#pragma unroll
+        for (int j = 0; j < VW; ++j) same &= w[j] == elem(i + j);
+      }
+    } else {
+      for (int i = 0; i < a.S && same; ++i) same = load_cg<W>(row + i) == elem(i);
+    }
     if (same) return INS_DUP;
     // the same fingerprint for another vector: keep probing
   }

@@ -58,3 +58,20 @@ def test_run_cli_and_batch_agree(tmp_path, oracle):
             pa, pb = infix_to_postfix(ea), infix_to_postfix(eb)
             assert len(pa) == len(pb)
             assert oracle.check(pb, inst.inputs, inst.outputs, 32)
+
+
+def test_compare_csvs(tmp_path):
+    """compare: agreement on found / not found and on expression size over the
+    instances both runs hold, and our expressions checked on their instances."""
+    ps = H.generate(tmp_path / "inst", size_range=(5, 5), var_range=(2, 2), repeats=3,
+                    samples=16, seed=3, bits=32)
+    insts = [Instance.read(p) for p in ps]
+    from simba_b200.instances import postfix_to_infix
+    a, b = tmp_path / "a.csv", tmp_path / "b.csv"
+    rows_a = [f"{p},{postfix_to_infix(i.formula)},0.1" for p, i in zip(ps, insts)]
+    rows_b = [f"{ps[0]},{postfix_to_infix(insts[0].formula)},0.5", f"{ps[1]},Not found !,0.5"]
+    a.write_text("instance,formula,time\n" + "\n".join(rows_a) + "\n")
+    b.write_text("instance,formula,time\n" + "\n".join(rows_b) + "\n")
+    r = H.compare(a, b)
+    assert r["common"] == 2 and r["agree_found"] == 1 and r["both_found"] == 1
+    assert r["agree_size"] == 1 and r["ours_found_verified"] == 2 and r["only_ours"] == 1
