@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the secondary objects (larger sweep, batch, VFB)")
-    ap.add_argument("--case", choices=["spine12", "spine13", "sweep13", "batch10", "vfb10"],
+    ap.add_argument("--case", choices=["spine12", "spine13", "sweep13", "batch10", "vfb10", "mlp"],
                     help="run one small profiling case instead of the benchmark (no JSON line)")
     return ap.parse_args()
 
@@ -92,6 +92,19 @@ def run_case(name: str) -> None:
             for _ in range(2):
                 r = ss.sweep(2, 13)
         print("sweep13", r.candidates, r.evaluated, r.kernel_ms)
+    elif name == "mlp":  # proposal training steps: the tensor-core GEMMs
+        from simba_b200 import guided as G
+        insts = list(iter_batch(256, 10 ** 6, sizes=range(3, 10), vars_=(1, 2, 3, 4),
+                                samples=(64,), word_bits=64))
+        p = G.Proposal(seed=0)
+        labels = np.arange(256, dtype=np.int32) % 64
+        for _ in range(3):
+            loss = p.train_step(insts, labels, 1e-3)
+        big = list(iter_batch(8192, 2 * 10 ** 6, sizes=range(5, 12), vars_=(1, 2, 3, 4),
+                              samples=(64,), word_bits=64))
+        probs = p.predict(big)  # first GEMM: 8192 x 512 x 8192
+        p.close()
+        print("mlp", loss, probs.shape)
     elif name == "batch10":
         insts = list(iter_batch(256, 5 * 10 ** 6, sizes=range(7, 20), vars_=(2, 3, 4, 5),
                                 samples=(32, 64, 128), word_bits=64))
@@ -362,7 +375,17 @@ def secondary(a, S, sess, inst, device: int, stream) -> dict:
         pass
     hbm = peaks.get("hbm_gbs")
     gbs = v2.bytes_moved / max(v2.device_ms / 1e3, 1e-9) / 1e9
+    inst32 = make_instance(TARGET_SIZE, N_VARS, N_SAMPLES, 1, word_bits=32, unsat=True)
+    S.vfb_solve(inst32, VFB_L, device=device, reference_dedup=True)
+    t0 = time.perf_counter()
+    v3 = S.vfb_solve(inst32, VFB_L, device=device, reference_dedup=True)
+    t_v3 = time.perf_counter() - t0
     out["vfb"] = {
+        "like_reference_u32_maxlen_10": {
+            "what": "reference uniqueness test as written, 32-bit words, the reference arm's "
+                    "vfb object runs the reference executable on the same file",
+            "status": v3.status, "candidates": v3.candidates, "rows": v3.rows_total,
+            "device_ms": v3.device_ms, "seconds": t_v3},
         "satisfiable": {"status": v1.status, "size": v1.size, "expr": v1.expr,
                         "device_ms": v1.device_ms, "candidates": v1.candidates,
                         "rows": v1.rows_total},
@@ -537,7 +560,40 @@ def run_reference(a, rank: int) -> None:
            "e2e": {"value": value, "unit": "candidate-evals/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0},
            "reference_seconds_per_step_incl_context": statistics.mean(steps)}
+    out["vfb"] = reference_vfb(a)
     print(json.dumps(out), flush=True)
+
+
+VFB_L = 10
+
+
+def reference_vfb(a) -> dict:
+    """The reference's VFB executable (vfb/src/full-cache.cu, rebuilt for
+    sm_100a, 32-bit words: it has no 64-bit path) on the 32-bit version of the
+    workload, unsatisfiable, to maxLen 10: its own printed seconds minus its
+    CUDA start-up (maxLen 1).  This repository's arm runs vfb_solve with the
+    reference's uniqueness test as written on the same file and maxLen."""
+    exe = ROOT / "oracle" / "_ref" / "vfb_full_cache"
+    if not exe.exists():
+        return {"unavailable": "oracle/_ref/vfb_full_cache missing"}
+    inst = make_workload(1, 32)
+    with tempfile.TemporaryDirectory() as td:
+        p = Path(td) / "vfb.json"
+        inst.write(p)
+
+        def once(max_len: int):
+            r = subprocess.run([str(exe), str(p), str(max_len)], capture_output=True, text=True,
+                               timeout=900)
+            line = r.stdout.strip().splitlines()[-1]
+            return line.rsplit(",", 2)[1], float(line.rsplit(",", 1)[1])
+
+        init = statistics.median([once(1)[1] for _ in range(3)])
+        once(VFB_L)
+        runs = [once(VFB_L) for _ in range(3)]
+    secs = statistics.median([t for _, t in runs])
+    return {"workload": f"u32 version of the workload, unsatisfiable, maxLen {VFB_L}",
+            "expr": runs[0][0], "seconds": max(secs - init, 1e-9),
+            "seconds_incl_context": secs, "startup_s": init}
 
 
 def main():

@@ -323,6 +323,14 @@ int simba_mlp_features(simba_mlp *mlp, const simba_instance *insts, int n, float
 int simba_mlp_get_params(simba_mlp *mlp, float *params);
 int simba_mlp_set_params(simba_mlp *mlp, const float *params);
 
+/* Device memory released by the calls above is kept in a process-wide cache
+ * (up to SIMBA_DEVICE_CACHE_BYTES, default 32 GiB per process, 0 = off) and
+ * reused by later calls, so that repeated searches do not allocate and free
+ * gigabytes of value tables each time (no counterpart in the reference,
+ * which allocates per run).  This returns every cached block to the device.
+ * Do not call it while another thread's call is running. */
+int simba_release_device_cache(void);
+
 const char *simba_version(void);
 const char *simba_status_string(int status);
 const char *simba_last_error(void);

@@ -395,6 +395,11 @@ def alu_peak(device: int = 0) -> float:
     return v.value
 
 
+def release_device_cache() -> None:
+    """Return the device memory the library keeps cached between calls."""
+    _check(lib().simba_release_device_cache())
+
+
 def device_count() -> int:
     return int(lib().simba_device_count())
 

@@ -3,13 +3,17 @@
 
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <map>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <vector>
 
 #include "../../include/simba_b200.h"
+#include "cuda_util.h"
 #include "engine.h"
 #include "grammar.h"
 #include "ext_grammar.h"
@@ -21,6 +25,97 @@ static thread_local std::string g_last_error;
 
 std::string last_error() { return g_last_error; }
 void set_last_error(const std::string& e) { g_last_error = e; }
+
+// ---------------------------------------------------------------- device cache
+
+namespace {
+struct DeviceCache {
+  std::mutex mu;
+  std::multimap<size_t, std::pair<int, void*>> blocks;  // bytes -> (device, pointer)
+  size_t cached = 0;
+  size_t cap = 0;
+};
+DeviceCache& cache() {
+  // created once, never destroyed: no cudaFree runs after the CUDA runtime
+  // has shut down at process exit
+  static DeviceCache* c = [] {
+    DeviceCache* d = new DeviceCache;
+    const char* e = getenv("SIMBA_DEVICE_CACHE_BYTES");
+    d->cap = e ? (size_t)strtoull(e, nullptr, 10) : (size_t)32 << 30;
+    return d;
+  }();
+  return *c;
+}
+// frees the cached blocks of one device (-1: all); the caller holds the lock
+void drop_cached(DeviceCache& c, int dev) {
+  int cur = -1;
+  cudaGetDevice(&cur);
+  for (auto it = c.blocks.begin(); it != c.blocks.end();) {
+    if (dev >= 0 && it->second.first != dev) {
+      ++it;
+      continue;
+    }
+    cudaSetDevice(it->second.first);
+    cudaFree(it->second.second);
+    c.cached -= it->first;
+    it = c.blocks.erase(it);
+  }
+  if (cur >= 0) cudaSetDevice(cur);
+}
+}  // namespace
+
+cudaError_t pool_alloc(void** p, size_t n, size_t* got) {
+  DeviceCache& c = cache();
+  int dev = 0;
+  cudaGetDevice(&dev);
+  {
+    std::lock_guard<std::mutex> g(c.mu);
+    // best fit on this device, at most twice the request
+    for (auto it = c.blocks.lower_bound(n); it != c.blocks.end() && it->first <= 2 * n + (1 << 20);
+         ++it) {
+      if (it->second.first != dev) continue;
+      *p = it->second.second;
+      *got = it->first;
+      c.cached -= it->first;
+      c.blocks.erase(it);
+      return cudaSuccess;
+    }
+  }
+  cudaError_t e = cudaMalloc(p, n);
+  if (e == cudaErrorMemoryAllocation) {  // give the cached blocks back and retry
+    cudaGetLastError();
+    {
+      std::lock_guard<std::mutex> g(c.mu);
+      drop_cached(c, dev);
+    }
+    e = cudaMalloc(p, n);
+  }
+  if (e == cudaSuccess) *got = n;
+  return e;
+}
+
+size_t pool_cached_bytes(int dev) {
+  DeviceCache& c = cache();
+  std::lock_guard<std::mutex> g(c.mu);
+  size_t n = 0;
+  for (const auto& b : c.blocks)
+    if (b.second.first == dev) n += b.first;
+  return n;
+}
+
+void pool_free(void* p, size_t bytes) {
+  if (!p) return;
+  DeviceCache& c = cache();
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> g(c.mu);
+  if (c.cached + bytes <= c.cap) {
+    c.blocks.emplace(bytes, std::make_pair(dev, p));
+    c.cached += bytes;
+    return;
+  }
+  cudaFree(p);
+}
 
 int validate(const HostInstance& h, int max_size) {
   if (h.bits != 32 && h.bits != 64) {
@@ -741,6 +836,13 @@ const char* simba_status_string(int status) {
 }
 
 const char* simba_last_error(void) { return g_last_error.c_str(); }
+
+int simba_release_device_cache(void) {
+  DeviceCache& c = cache();
+  std::lock_guard<std::mutex> g(c.mu);
+  drop_cached(c, -1);
+  return 0;
+}
 
 int simba_device_count(void) {
   int n = 0;

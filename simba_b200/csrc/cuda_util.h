@@ -19,7 +19,19 @@ void set_last_error(const std::string& e);
     }                                                                              \
   } while (0)
 
-// Device allocation owned by the host object; freed on destruction.
+// Process-wide cache of device allocations (capi.cpp): a buffer released by
+// one call is handed to the next call that needs one of about its size, so
+// that repeated searches do not pay cudaMalloc / cudaFree for gigabytes of
+// value tables every time.  Blocks are cached only after the work that used
+// them has been synchronised (every engine synchronises before it releases
+// its buffers); the cache is capped (SIMBA_DEVICE_CACHE_BYTES, default
+// 32 GiB, 0 = off) and emptied by simba_release_device_cache and, for a
+// device, whenever a cudaMalloc there runs out of memory.
+cudaError_t pool_alloc(void** p, size_t n, size_t* got);
+void pool_free(void* p, size_t bytes);
+size_t pool_cached_bytes(int device);  // bytes the cache holds on a device
+
+// Device allocation owned by the host object; released on destruction.
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
@@ -28,7 +40,7 @@ struct DevBuf {
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) pool_free(p, bytes);
     p = nullptr;
     bytes = 0;
   }
@@ -36,8 +48,9 @@ struct DevBuf {
   cudaError_t reserve(size_t n) {
     if (n <= bytes) return cudaSuccess;
     release();
-    cudaError_t e = cudaMalloc(&p, n);
-    if (e == cudaSuccess) bytes = n;
+    size_t got = 0;
+    cudaError_t e = pool_alloc(&p, n, &got);
+    if (e == cudaSuccess) bytes = got;
     else p = nullptr;
     return e;
   }

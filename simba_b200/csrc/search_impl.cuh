@@ -69,6 +69,12 @@ constexpr int kPreG = 131072;  // the same queue per CTA in global memory, when 
 #ifndef SIMBA_KR
 #define SIMBA_KR 8
 #endif
+#ifndef SIMBA_NESTED_PIPELINE
+#define SIMBA_NESTED_PIPELINE 1  // nested compares: next loads issued before the current tests
+#endif
+#ifndef SIMBA_JOIN_VALS_LOG2
+#define SIMBA_JOIN_VALS_LOG2 15  // hash join: bottom values per work unit
+#endif
 // Resident CTAs per SM the spine kernel is compiled for: 3 caps it at 85
 // registers (80 used, a few hundred bytes of spills), the occupancy its work
 // units were tuned at; left to itself the compiler picked 48 registers and
@@ -91,7 +97,7 @@ constexpr int kExtra = 3;       // samples besides sample 0 with value tables (m
 constexpr int kJoinCtx = 512;
 constexpr int kJoinSlots = 1024;
 constexpr int kJoinBits = 16384;
-constexpr unsigned long long kJoinVals = 1ULL << 15;
+constexpr unsigned long long kJoinVals = 1ULL << SIMBA_JOIN_VALS_LOG2;
 constexpr unsigned long long kJoinMin = 1;
 
 // One level of a spine, top-down (level 0 is the root).
@@ -723,19 +729,21 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
     W xs[VW];
     memcpy(xs, &raw, 16);
     bool hit = false;
+    // independent accumulators: the or-chains of the contexts run in parallel
     if (PACK && use_pack) {
-      unsigned acc = 0;
+      unsigned acc[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
       for (int e = 0; e < VW; e += 2) {
         const unsigned yp = __byte_perm((unsigned)xs[e], (unsigned)xs[e + 1], 0x5410);
 #pragma unroll
         for (int r = 0; r < kR; ++r) {
           const unsigned z = (yp & Mp[r]) ^ Kp[r];
-          acc |= (z - 0x00010001u) & ~z;
+          acc[r & 3] |= (z - 0x00010001u) & ~z;
         }
       }
-      hit = (acc & 0x80008000u) != 0;
+      hit = ((acc[0] | acc[1] | acc[2] | acc[3]) & 0x80008000u) != 0;
     } else {
+      bool h4[4] = {false, false, false, false};
 #pragma unroll
       for (int e = 0; e < VW; ++e) {
 #pragma unroll
@@ -747,9 +755,10 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
             for (int j = 0; j < EE; ++j) wh[j] = (H)WX[r][j];
             y = eval_explicit<H, E>(XH, wh, y);
           }
-          hit |= FULL ? (y == (H)K[r]) : ((H)(y & (H)M[r]) == (H)K[r]);
+          h4[r & 3] |= FULL ? (y == (H)K[r]) : ((H)(y & (H)M[r]) == (H)K[r]);
         }
       }
+      hit = h4[0] | h4[1] | h4[2] | h4[3];
     }
     if (!hit) return;
     for (int e = 0; e < VW; ++e) {
@@ -770,6 +779,31 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
   unsigned long long q = q0 + lane;
   const unsigned long long step = (unsigned long long)L;
   if (E == 0) {
+#if SIMBA_NESTED_PIPELINE
+    // software pipeline: the next four loads are issued before the current
+    // four are tested, so the tests overlap their latency
+    if (q + 3 * step < q1) {
+      uint4 a0 = __ldg(V4 + q), a1 = __ldg(V4 + q + step);
+      uint4 a2 = __ldg(V4 + q + 2 * step), a3 = __ldg(V4 + q + 3 * step);
+      for (; q + 7 * step < q1; q += 4 * step) {
+        const uint4 b0 = __ldg(V4 + q + 4 * step), b1 = __ldg(V4 + q + 5 * step);
+        const uint4 b2 = __ldg(V4 + q + 6 * step), b3 = __ldg(V4 + q + 7 * step);
+        test(a0, q);
+        test(a1, q + step);
+        test(a2, q + 2 * step);
+        test(a3, q + 3 * step);
+        a0 = b0;
+        a1 = b1;
+        a2 = b2;
+        a3 = b3;
+      }
+      test(a0, q);
+      test(a1, q + step);
+      test(a2, q + 2 * step);
+      test(a3, q + 3 * step);
+      q += 4 * step;
+    }
+#else
     for (; q + 3 * step < q1; q += 4 * step) {
       const uint4 a0 = __ldg(V4 + q);
       const uint4 a1 = __ldg(V4 + q + step);
@@ -780,6 +814,7 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
       test(a2, q + 2 * step);
       test(a3, q + 3 * step);
     }
+#endif
   }
   for (; q < q1; q += step) test(__ldg(V4 + q), q);
 }
@@ -921,12 +956,17 @@ __device__ void process_unit_join(const Params<W>& p, const InstDesc<W>& d, Smem
   }
   __syncthreads();
   const unsigned long long mc = js.mc;
+  // the block joins on at least the low 32 bits (every mask keeps them: the
+  // usual case): the hash reads the low word alone, and the exact key
+  // compare on a filter hit settles the rest (same hash as join_hash for
+  // 32-bit words)
+  const bool lo32 = sizeof(W) == 4 || (unsigned)mc == 0xFFFFFFFFu;
   // 2. filter bits and table entries, keyed on K & Mc
 #pragma unroll
   for (int r = 0; r < 2; ++r) {
     if (!ok[r]) continue;
     const int j = threadIdx.x + r * blockDim.x;
-    const unsigned hx = join_hash((unsigned long long)ks[r] & mc);
+    const unsigned hx = lo32 ? (unsigned)ks[r] * 0x85EBCA6Bu : join_hash((unsigned long long)ks[r] & mc);
     atomicOr(&js.bits[hx >> 23], 1u << ((hx >> 18) & 31));
     unsigned h = hx >> 22;
     for (int t = 0; t < kJoinSlots; ++t, h = (h + 1) & (kJoinSlots - 1)) {
@@ -951,9 +991,9 @@ __device__ void process_unit_join(const Params<W>& p, const InstDesc<W>& d, Smem
     for (int e = 0; e < VW; ++e) {
       const unsigned long long v = q * VW + e;
       const unsigned long long y = (unsigned long long)xs[e];
-      const unsigned long long ym = y & mc;
-      const unsigned hx = join_hash(ym);
+      const unsigned hx = lo32 ? (unsigned)y * 0x85EBCA6Bu : join_hash(y & mc);
       if (!(js.bits[hx >> 23] >> ((hx >> 18) & 31) & 1u)) continue;
+      const unsigned long long ym = y & mc;
       unsigned h = hx >> 22;
       for (int t = 0; t < kJoinSlots; ++t, h = (h + 1) & (kJoinSlots - 1)) {
         const unsigned c = js.ctx[h];
@@ -1272,15 +1312,22 @@ struct BuildJob {
 
 template <class W>
 __global__ void build_batch_kernel(const BuildJob<W>* jobs, int njobs, unsigned long long total) {
+  int cur = -1;  // the last job found: a thread's strided entries stay in it for a while
+  unsigned long long cur_lo = 1, cur_hi = 0;
   for (unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
        g += (unsigned long long)gridDim.x * blockDim.x) {
-    int lo = 0, hi = njobs - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (jobs[mid].begin <= g) lo = mid;
-      else hi = mid - 1;
+    if (g < cur_lo || g >= cur_hi) {
+      int lo = 0, hi = njobs - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].begin <= g) lo = mid;
+        else hi = mid - 1;
+      }
+      cur = lo;
+      cur_lo = jobs[lo].begin;
+      cur_hi = lo + 1 < njobs ? jobs[lo + 1].begin : total;
     }
-    const BuildJob<W>& j = jobs[lo];
+    const BuildJob<W>& j = jobs[cur];
     const unsigned long long i = g - j.begin;
     if (is_unary(j.op)) {
       j.out[i] = un_apply<W>(j.op, j.A[i]);
@@ -1813,6 +1860,9 @@ class Search final : public SearchSession {
     for (int s = built_ + 1; s <= t; ++s) {
       const int copies = s <= Tf_ ? nsamp() : 1;
       SB_CUDA(d_tabs_[s].reserve(padded(ct_.n[s][8]) * sizeof(W) * copies));
+      // one launch per size: every operator block of every sample's table
+      std::vector<BuildJob<W>> jobs;
+      uint64_t total = 0;
       for (int j = 0; j < copies; ++j) {
         W* o = tab(s, j);
         if (s == 1) {
@@ -1824,25 +1874,41 @@ class Search final : public SearchSession {
         uint64_t off = 0;
         const int sub = s - 1;
         for (int op = 0; op < 8; ++op) {
-          if (is_unary(op)) {
-            const uint64_t n = ct_.n[sub][8];
-            const int blocks = (int)std::min<uint64_t>((n + 255) / 256, (uint64_t)sms_ * 16);
-            build_unary_kernel<W><<<blocks, 256, 0, stream_>>>(o + off, tab(sub, j), n, op);
-            ++launches_;
-            off += n;
-            continue;
-          }
-          const int fmax = is_commutative(op) ? sub / 2 : sub - 1;
+          const int fmax = is_unary(op) ? 1 : (is_commutative(op) ? sub / 2 : sub - 1);
           for (int f = 1; f <= fmax; ++f) {
-            const uint64_t na = ct_.n[f][8], nb = ct_.n[sub - f][8];
-            const uint64_t n = na * nb;
-            const int blocks = (int)std::min<uint64_t>((n + 255) / 256, (uint64_t)sms_ * 16);
-            build_binary_kernel<W><<<blocks, 256, 0, stream_>>>(o + off, tab(f, j), tab(sub - f, j),
-                                                               na, nb, op);
-            ++launches_;
+            BuildJob<W> b;
+            memset(&b, 0, sizeof(b));
+            b.out = o + off;
+            b.op = op;
+            b.begin = total;
+            if (is_unary(op)) {
+              b.A = tab(sub, j);
+              b.na = ct_.n[sub][8];
+              b.nb = 1;
+            } else {
+              b.A = tab(f, j);
+              b.B = tab(sub - f, j);
+              b.na = ct_.n[f][8];
+              b.nb = ct_.n[sub - f][8];
+            }
+            const uint64_t n = b.na * b.nb;
+            if (n == 0) continue;
+            jobs.push_back(b);
             off += n;
+            total += n;
           }
         }
+      }
+      if (!jobs.empty()) {
+        // stream order keeps the previous size's build ahead of this copy;
+        // the copy from pageable memory is staged before the call returns
+        SB_CUDA(d_jobs_.reserve(jobs.size() * sizeof(BuildJob<W>)));
+        SB_CUDA(cudaMemcpyAsync(d_jobs_.p, jobs.data(), jobs.size() * sizeof(BuildJob<W>),
+                                cudaMemcpyHostToDevice, stream_));
+        const int blocks = (int)std::min<uint64_t>((total + 255) / 256, (uint64_t)sms_ * 16);
+        build_batch_kernel<W><<<blocks, 256, 0, stream_>>>(d_jobs_.as<BuildJob<W>>(), (int)jobs.size(),
+                                                            total);
+        ++launches_;
       }
       SB_CUDA(cudaGetLastError());
       built_ = s;
@@ -2179,7 +2245,7 @@ class Search final : public SearchSession {
   uint64_t alg_ops_ = 0;
   int sms_ = 0, grid_ = 0, grid_naive_ = 0, grid_join_ = 0;
   size_t smem_bytes_ = 0, join_off_ = 0, smem_join_ = 0;
-  DevBuf d_in_, d_out_, d_counts_, d_scal_, d_items_, d_small_, d_ctx_, d_insts_, d_preq_;
+  DevBuf d_in_, d_out_, d_counts_, d_scal_, d_items_, d_small_, d_ctx_, d_insts_, d_preq_, d_jobs_;
   DevBuf d_tabs_[kMaxSize + 1];  // V_t of every sample, allocated when size t is first built
   unsigned long long h_scal_[8] = {};
   int Tcap_ = 0, Tf_ = 0, built_ = 0, last_T_ = 0;
@@ -2477,7 +2543,7 @@ class Batch {
       // instances of the round wait for a later round if they do not
       size_t mem_free = 0, mem_total = 0;
       SB_CUDA(cudaMemGetInfo(&mem_free, &mem_total));
-      const uint64_t room = mem_free + d_ctx_.bytes;
+      const uint64_t room = mem_free + d_ctx_.bytes + pool_cached_bytes(o_.device);
       const uint64_t ctx_room = room > (1ULL << 30) ? (room - (1ULL << 30)) / sizeof(Ctx<W>) : 0;
       for (int i : order) {
         ran[i] = 0;
