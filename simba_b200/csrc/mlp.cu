@@ -12,7 +12,7 @@
 //             Z3 = H2 W3 + b3, p = softmax(Z3), loss = mean cross-entropy.
 //   GEMMs     BF16 operands, FP32 accumulation, tcgen05.mma on the
 //             5th-generation tensor cores with the accumulator in TMEM
-//             (128x64 CTA tiles, gemm_tc_kernel).
+//             (128x128 CTA tiles, two-stage cp.async pipeline, gemm_tc_kernel).
 //   training  hand-written backward pass and Adam (FP32 master weights,
 //             BF16 copies feed the GEMMs).
 #include <cuda_bf16.h>
@@ -71,18 +71,22 @@ __global__ void features_kernel(const unsigned long long* in, const unsigned lon
 // C[M x N] = A[M x K] * Bt[N x K]^T (+ bias[n]) on the 5th-generation tensor
 // cores: tcgen05.mma (kind::f16, BF16 operands, FP32 accumulation in TMEM),
 // one elected thread issuing, the accumulator read back with tcgen05.ld.
-//   * One CTA (4 warps) per 128 x 64 tile of C; K in steps of 64.
+//   * One CTA (4 warps) per 128 x 128 tile of C; K in steps of 64.
 //   * Operands are staged in shared memory in the canonical K-major layout
 //     without swizzle: 8 x 8 core matrices of 128 contiguous bytes (8 rows of
 //     16 bytes), core matrix (row group i, k group j) at (8 i + j) * 128, so
 //     the leading (K) byte offset is 128 and the stride (M/N) byte offset is
 //     1024; each MMA covers K = 16, i.e. two k groups (+256 bytes).
-//   * tcgen05.commit arrives on an mbarrier when the MMAs of a step are done;
-//     every wait is bounded and reports through *err.
+//   * Two stages: the asynchronous copies (cp.async, zero-filled past the
+//     matrix edges) of step k+1 run while the MMAs of step k do; a stage is
+//     refilled only after tcgen05.commit has signalled (mbarrier) that the
+//     MMAs reading it are done.  Every wait is bounded and reports through
+//     *err.
 // Both operands are K-major (row stride lda / ldb elements, multiples of 8,
 // 16-byte aligned rows); the caller transposes where needed.
-constexpr int kTcM = 128, kTcN = 64, kTcK = 64;
-constexpr size_t kTcSmem = 48 * 1024;  // 24 KB of tiles; 48 KB keeps <= 4 CTAs (256 TMEM columns) per SM
+constexpr int kTcM = 128, kTcN = 128, kTcK = 64, kTcStages = 2;
+constexpr int kTcTileA = kTcM * kTcK * 2, kTcTileB = kTcN * kTcK * 2;
+constexpr size_t kTcSmem = kTcStages * (kTcTileA + kTcTileB) + 1024;  // 3 CTAs (384 TMEM columns) per SM
 
 __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
   uint64_t d = 0;
@@ -103,24 +107,23 @@ __device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t phase) {
   return false;
 }
 
-// rows [r0, r0 + nrows) x k [k0, k0 + 64) of a K-major matrix into the canonical tile
-__device__ __forceinline__ void tc_stage(uint8_t* tile, const bf16* G, int ld, int r0, int nrows_total,
+// rows [r0, r0 + rows) x k [k0, k0 + 64) of a K-major matrix into the
+// canonical tile at shared address `tile`, by 16-byte asynchronous copies;
+// bytes past row nrows_total or column K are zero-filled
+__device__ __forceinline__ void tc_stage(uint32_t tile, const bf16* G, int ld, int r0, int nrows_total,
                                          int rows, int k0, int K) {
   for (int c = threadIdx.x; c < rows * 8; c += blockDim.x) {
     const int row = c >> 3, kc = c & 7;
     const int gr = r0 + row, gk = k0 + kc * 8;
-    uint4 v = make_uint4(0, 0, 0, 0);
-    if (gr < nrows_total) {
-      const bf16* src = G + (size_t)gr * ld + gk;
-      if (gk + 8 <= K) {
-        v = *reinterpret_cast<const uint4*>(src);
-      } else if (gk < K) {
-        __align__(16) bf16 e[8];
-        for (int q = 0; q < 8; ++q) e[q] = gk + q < K ? src[q] : __float2bfloat16(0.f);
-        v = *reinterpret_cast<const uint4*>(e);
-      }
+    const bf16* src = G;
+    int bytes = 0;
+    if (gr < nrows_total && gk < K) {
+      src = G + (size_t)gr * ld + gk;
+      bytes = (K - gk < 8 ? K - gk : 8) * 2;
     }
-    *reinterpret_cast<uint4*>(tile + ((row >> 3) * 8 + kc) * 128 + (row & 7) * 16) = v;
+    const uint32_t dst = tile + (uint32_t)(((row >> 3) * 8 + kc) * 128 + (row & 7) * 16);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"(dst), "l"(src), "r"(bytes)
+                 : "memory");
   }
 }
 
@@ -128,19 +131,25 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(int M, int N, int K, const
                                                       const bf16* Bt, int ldb, float* C, int ldc,
                                                       const float* bias, int* err) {
   extern __shared__ __align__(1024) uint8_t tc_smem[];
-  uint8_t* sA = tc_smem;
-  uint8_t* sB = tc_smem + kTcM * kTcK * 2;
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t mbar[kTcStages];
   __shared__ uint32_t tmem_base;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&mbar);
+  const uint32_t base = ((uint32_t)__cvta_generic_to_shared(tc_smem) + 1023u) & ~1023u;
+  uint32_t sA[kTcStages], sB[kTcStages], mb[kTcStages];
+#pragma unroll
+  for (int s = 0; s < kTcStages; ++s) {
+    sA[s] = base + (uint32_t)(s * (kTcTileA + kTcTileB));
+    sB[s] = sA[s] + (uint32_t)kTcTileA;
+    mb[s] = (uint32_t)__cvta_generic_to_shared(&mbar[s]);
+  }
   if (warp == 0) {
     const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&tmem_base);
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" :: "r"(dst));
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" :: "r"(dst));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (threadIdx.x == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(mb));
+#pragma unroll
+    for (int s = 0; s < kTcStages; ++s) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(mb[s]));
     asm volatile("fence.mbarrier_init.release.cluster;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -151,37 +160,55 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(int M, int N, int K, const
   // kind::f16 instruction descriptor: FP32 D, BF16 A and B, both K-major, N, M
   const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
                          ((uint32_t)(kTcM >> 4) << 24);
-  uint32_t phase = 0;
+  const int nk = (K + kTcK - 1) / kTcK;
+  uint32_t ph[kTcStages] = {0u, 0u};
   bool ok = true;
-  for (int k0 = 0; k0 < K && ok; k0 += kTcK) {
-    tc_stage(sA, A, lda, m0, M, kTcM, k0, K);
-    tc_stage(sB, Bt, ldb, n0, N, kTcN, k0, K);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // st.shared -> tensor core
+  tc_stage(sA[0], A, lda, m0, M, kTcM, 0, K);
+  tc_stage(sB[0], Bt, ldb, n0, N, kTcN, 0, K);
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  for (int k = 0; k < nk && ok; ++k) {
+    const int s = k & 1;
+    if (k + 1 < nk) {
+      if (k >= 1) {  // stage s^1 was read by the MMAs of step k-1
+        // one verdict for the whole CTA, so that every thread leaves together
+        if (__syncthreads_or(tc_wait(mb[s ^ 1], ph[s ^ 1]) ? 0 : 1)) {
+          ok = false;
+          if (threadIdx.x == 0) atomicOr(err, 1);
+          break;
+        }
+        ph[s ^ 1] ^= 1u;
+      }
+      tc_stage(sA[s ^ 1], A, lda, m0, M, kTcM, (k + 1) * kTcK, K);
+      tc_stage(sB[s ^ 1], Bt, ldb, n0, N, kTcN, (k + 1) * kTcK, K);
+      asm volatile("cp.async.commit_group;" ::: "memory");
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // copies -> tensor core
     __syncthreads();
     if (threadIdx.x == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;");
-      const uint32_t a0 = (uint32_t)__cvta_generic_to_shared(sA);
-      const uint32_t b0 = (uint32_t)__cvta_generic_to_shared(sB);
 #pragma unroll
       for (int kk = 0; kk < kTcK / 16; ++kk) {
-        const uint64_t ad = tc_desc(a0 + kk * 256), bd = tc_desc(b0 + kk * 256);
-        const uint32_t accumulate = (k0 > 0 || kk > 0) ? 1u : 0u;
+        const uint64_t ad = tc_desc(sA[s] + kk * 256), bd = tc_desc(sB[s] + kk * 256);
+        const uint32_t accumulate = (k > 0 || kk > 0) ? 1u : 0u;
         asm volatile("{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
                      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
                      :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(accumulate));
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                   :: "r"(mb) : "memory");
+                   :: "r"(mb[s]) : "memory");
     }
     __syncwarp();
-    if (!tc_wait(mb, phase)) {  // the tiles stay in use until the MMAs are done
-      ok = false;
-      atomicOr(err, 1);
-    }
-    phase ^= 1;
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    __syncthreads();
   }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  // the last commit covers every MMA issued before it
+  if (ok && __syncthreads_or(tc_wait(mb[(nk - 1) & 1], ph[(nk - 1) & 1]) ? 0 : 1)) {
+    ok = false;
+    if (threadIdx.x == 0) atomicOr(err, 1);
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;");
   if (ok) {  // warp w owns TMEM lanes (rows) 32 w .. 32 w + 31
     const int row = m0 + warp * 32 + lane;
 #pragma unroll
@@ -205,7 +232,7 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(int M, int N, int K, const
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" :: "r"(tmem));
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" :: "r"(tmem));
 }
 
 // out[c][r] = in[r][c] for a rows x cols BF16 matrix; out rows are ldo

@@ -70,7 +70,10 @@ constexpr int kPreG = 131072;  // the same queue per CTA in global memory, when 
 #define SIMBA_KR 8
 #endif
 #ifndef SIMBA_NESTED_PIPELINE
-#define SIMBA_NESTED_PIPELINE 1  // nested compares: next loads issued before the current tests
+#define SIMBA_NESTED_PIPELINE 0  // nested compares: next loads issued before the current tests
+#endif                           // (measured: no gain at 3 CTAs/SM, the extra registers spill)
+#ifndef SIMBA_PACK_IMAD
+#define SIMBA_PACK_IMAD 1  // packed prefilter: the subtraction as a multiply-add (FMA pipe)
 #endif
 #ifndef SIMBA_JOIN_VALS_LOG2
 #define SIMBA_JOIN_VALS_LOG2 15  // hash join: bottom values per work unit
@@ -248,7 +251,8 @@ struct alignas(16) Smem {
   Item item;  // 16-byte aligned: filled with uint4 copies
   alignas(16) unsigned char desc[sizeof(InstDesc<unsigned long long>)];
   int inst_idx;
-  int pad_[3];
+  unsigned one;  // 1, read back so that the compiler cannot fold it (see process_unit)
+  int pad_[2];
   unsigned long long queue[kQueue];
   unsigned long long pre_c[kPre], pre_v[kPre];  // sample-0 matches: context, bottom index
   int pn;
@@ -725,6 +729,10 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
     }
     use_pack = __all_sync(0xFFFFFFFFu, dense);
   }
+  // z - 0x00010001 as z * one + 0xFFFEFFFF with `one` unknown to the
+  // compiler: a multiply-add, which runs on the FMA pipe, so that the ALU
+  // pipe keeps only the two bitwise operations of each context test
+  const unsigned one = SIMBA_PACK_IMAD ? *(volatile unsigned*)&sm.one : 1u;
   auto test = [&](const uint4& raw, unsigned long long q) {
     W xs[VW];
     memcpy(xs, &raw, 16);
@@ -738,7 +746,7 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
 #pragma unroll
         for (int r = 0; r < kR; ++r) {
           const unsigned z = (yp & Mp[r]) ^ Kp[r];
-          acc[r & 3] |= (z - 0x00010001u) & ~z;
+          acc[r & 3] |= (z * one + 0xFFFEFFFFu) & ~z;
         }
       }
       hit = ((acc[0] | acc[1] | acc[2] | acc[3]) & 0x80008000u) != 0;
@@ -1095,6 +1103,7 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
   JoinSmem* js = p.join_off ? reinterpret_cast<JoinSmem*>(smem_raw + p.join_off) : nullptr;
   const InstDesc<W>& d = *reinterpret_cast<const InstDesc<W>*>(sm.desc);
   if (threadIdx.x == 0) {
+    sm.one = 1u;
     sm.qn = 0;
     sm.pn = 0;
     sm.item_idx = -1;
