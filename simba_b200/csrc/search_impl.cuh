@@ -72,6 +72,9 @@ constexpr int kPreG = 131072;  // the same queue per CTA in global memory, when 
 #ifndef SIMBA_NESTED_PIPELINE
 #define SIMBA_NESTED_PIPELINE 0  // nested compares: next loads issued before the current tests
 #endif                           // (measured: no gain at 3 CTAs/SM, the extra registers spill)
+#ifndef SIMBA_PACK_ALWAYS
+#define SIMBA_PACK_ALWAYS 0  // packed prefilter in every warp (for comparisons)
+#endif
 #ifndef SIMBA_PACK_IMAD
 #define SIMBA_PACK_IMAD 1  // packed prefilter: the subtraction as a multiply-add (FMA pipe)
 #endif
@@ -710,24 +713,27 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
   // nonzero half never does, and borrows cannot cross from a nonzero low
   // half).  One subtraction and two bitwise operations test two candidates.
   // A 16-bit window passes a random value with probability 2^-(mask bits in
-  // it), so the packed test only pays where every context of the warp keeps
-  // at least kPackMinBits low mask bits; other warps (sparse masks, e.g. an &
-  // with a small value that has few bits set) take the 32-bit test, whose
-  // survivors are rarer.  The choice is uniform across the warp.
+  // it): a thread's 16-bit tests of one 16-byte load (2 values x kR
+  // contexts) let something through with probability about
+  // 2 * sum_r 2^-bits_r, and a pass costs the 32-bit tests of those
+  // candidates.  The packed test pays while that probability stays under
+  // ~0.25 (16 bitwise operations instead of 32 per load, plus the passes);
+  // warps with a thread above it (sparse masks, e.g. an & with a small value
+  // of few bits) take the 32-bit test throughout.  The choice is uniform
+  // across the warp.
   constexpr bool PACK = SIMBA_NESTED_PACK16 && E == 0 && !FULL;
-  constexpr int kPackMinBits = 10;
   unsigned Mp[PACK ? kR : 1], Kp[PACK ? kR : 1];
   bool use_pack = false;
   if (PACK) {
-    bool dense = true;
+    float pass = 0.f;
 #pragma unroll
     for (int r = 0; r < kR; ++r) {
       const unsigned m16 = (unsigned)M[r] & 0xFFFFu, k16 = (unsigned)K[r] & 0xFFFFu;
       Mp[r] = m16 | (m16 << 16);
       Kp[r] = k16 | (k16 << 16);
-      dense &= __popc(m16) >= kPackMinBits;
+      pass += __int_as_float((127 - __popc(m16)) << 23);  // 2^-bits
     }
-    use_pack = __all_sync(0xFFFFFFFFu, dense);
+    use_pack = SIMBA_PACK_ALWAYS || __all_sync(0xFFFFFFFFu, 2.f * pass < 0.25f);
   }
   // z - 0x00010001 as z * one + 0xFFFEFFFF with `one` unknown to the
   // compiler: a multiply-add, which runs on the FMA pipe, so that the ALU
