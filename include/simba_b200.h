@@ -130,6 +130,9 @@ typedef struct {
                             table once per block of contexts                    */
   double join_table_bytes;    /* the bottom tables the join launches read, each
                             counted once per size: the algorithmic minimum     */
+  uint64_t nested_live_candidates; /* nested-compare candidates whose context can
+                            match sample 0 and were compared one by one; the
+                            rest were decided by their context's constraint   */
 } simba_result;
 
 /* Plain cache-free unranking search of one instance: replaces NoCache::solve

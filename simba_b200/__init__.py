@@ -86,7 +86,8 @@ class _Result(C.Structure):
                 ("launches", C.c_int32), ("kernel_ms", C.c_double), ("alg_ops", C.c_uint64),
                 ("join_ms", C.c_double), ("nested_ms", C.c_double),
                 ("join_candidates", C.c_uint64), ("nested_candidates", C.c_uint64),
-                ("join_bytes_streamed", C.c_double), ("join_table_bytes", C.c_double)]
+                ("join_bytes_streamed", C.c_double), ("join_table_bytes", C.c_double),
+                ("nested_live_candidates", C.c_uint64)]
 
 
 _lib = None
@@ -154,6 +155,7 @@ class Result:
     nested_candidates: int = 0
     join_bytes_streamed: float = 0.0
     join_table_bytes: float = 0.0
+    nested_live_candidates: int = 0
 
     @property
     def found(self) -> bool:
@@ -165,7 +167,7 @@ def _res(r: _Result) -> Result:
                   r.seconds, r.device_ms, r.candidates, r.evaluated, list(r.per_size),
                   r.table_size, r.max_size_searched, r.launches, r.kernel_ms, r.alg_ops,
                   r.join_ms, r.nested_ms, r.join_candidates, r.nested_candidates,
-                  r.join_bytes_streamed, r.join_table_bytes)
+                  r.join_bytes_streamed, r.join_table_bytes, r.nested_live_candidates)
 
 
 class _Arrays:

@@ -279,6 +279,7 @@ static void fill_result(const SolveOutcome& oc, double secs, simba_result* r, in
   r->nested_candidates = oc.nested_candidates;
   r->join_bytes_streamed = oc.join_bytes_streamed;
   r->join_table_bytes = oc.join_table_bytes;
+  r->nested_live_candidates = oc.nested_live_candidates;
 }
 
 int read_instance_json(const std::string& path, HostInstance* h) {

@@ -57,6 +57,7 @@ struct SolveOutcome {
   // the two launch kinds of the spine kernel (single-instance searches)
   double join_ms = 0.0, nested_ms = 0.0;
   uint64_t join_candidates = 0, nested_candidates = 0;
+  uint64_t nested_live_candidates = 0;  // of those, candidates of contexts that can match
   double join_bytes_streamed = 0.0, join_table_bytes = 0.0;
 };
 

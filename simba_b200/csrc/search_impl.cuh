@@ -61,6 +61,7 @@ constexpr int kQueue = 128;    // shared-memory queue of matches to verify
 constexpr int kPre = 256;      // shared-memory queue of sample-0 matches to filter
 constexpr int kPreG = 131072;  // the same queue per CTA in global memory, when given
                                // (8-byte entries: context << 32 | bottom index)
+constexpr int kLive = 512;     // live contexts of a nested-compare unit listed in shared memory
 // Tuning knobs (compile-time): contexts per thread, minimum resident CTAs
 // per SM.
 #ifndef SIMBA_NESTED_PACK16
@@ -238,6 +239,7 @@ struct Params {
   unsigned long long* start_ns;
   int* flags;  // [0] budget expired, [1] inversion failure, [2] queue overflows
   unsigned long long* hits;  // sample-0 matches sent to verification (may be null)
+  unsigned long long* live;  // candidates of live nested-compare contexts (may be null)
   unsigned long long* preq;  // per-CTA queues of sample-0 matches, [grid][kPreG] (may be null)
   unsigned join_off;         // byte offset of JoinSmem in dynamic shared memory; 0: no join units
   unsigned long long total_units;
@@ -259,6 +261,8 @@ struct alignas(16) Smem {
   unsigned long long queue[kQueue];
   unsigned long long pre_c[kPre], pre_v[kPre];  // sample-0 matches: context, bottom index
   int pn;
+  int nlive;                   // live contexts of the current nested-compare unit
+  unsigned short live[kLive];  // their offsets from the unit's first context
   unsigned long long unit;
   unsigned long long unit_local;  // unit index within its spine
   int qn;
@@ -635,6 +639,31 @@ __device__ void filter_queue(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
   }
 }
 
+// Sample-0 constraint (v & M) == K on the bottom value of context c, from the
+// levels the inversion absorbs; the small values of the explicit levels go
+// to wx.  M = 0 with K != 0: no bottom value can match.
+template <class W, int E, bool FUSED>
+__device__ __forceinline__ void context_constraint(const Params<W>& p, const InstDesc<W>& d,
+                                                   const Item& it, unsigned long long c, W& m, W& k,
+                                                   W* wx) {
+  if (FUSED) {
+    const Ctx<W> cx = p.ctxs[it.ctx_off + c];
+    m = cx.M;
+    k = cx.K;
+    return;
+  }
+  W wl[kMaxDepth];
+  decode_context<W>(d, it, c, wl);
+  m = (W)~W(0);
+  k = d.target;
+  for (int l = 0; l < it.inv; ++l)
+    if (!invert_level<W>(it.lv[l], wl[l], m, k)) atomicOr(&p.flags[1], 1);
+  if (E > 0 && wx) {
+#pragma unroll
+    for (int j = 0; j < (E > 0 ? E : 1); ++j) wx[j] = wl[it.inv + j];
+  }
+}
+
 template <class W, int E, bool FULL, bool FUSED>
 __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm, const Item& it,
                              unsigned long long local, const W* s_in, const W* s_out) {
@@ -642,9 +671,40 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
   constexpr int EE = E > 0 ? E : 1;
   const unsigned long long cblk = local / it.vblocks;
   const unsigned long long vblk = local - cblk * it.vblocks;
-  const int L = it.L;
-  const int g = threadIdx.x / L, lane = threadIdx.x - (threadIdx.x / L) * L;
-  const unsigned long long c0 = cblk * it.cb + (unsigned long long)g * kR;
+  const unsigned long long cbase = cblk * it.cb;  // the unit's first context
+  const unsigned ncu = (unsigned)umin64(it.cb, it.nctx - cbase);
+
+  // Contexts that no bottom value can complete to a sample-0 match (the
+  // inversion ended with M = 0, K != 0: an & whose small value lacks a bit
+  // the constraint needs, an | that sets a bit it must not) are decided here
+  // without reading the bottom table; on random targets most contexts under
+  // an & or | are such.  The live ones are listed in shared memory and, when
+  // the list holds them all, the CTA's threads are laid out over them alone:
+  // ceil(live / kR) groups, the rest of the threads as value lanes.
+  if (threadIdx.x == 0) sm.nlive = 0;
+  __syncthreads();
+  for (unsigned j = threadIdx.x; j < ncu; j += blockDim.x) {
+    W m, k;
+    context_constraint<W, E, FUSED>(p, d, it, cbase + j, m, k, nullptr);
+    if (!(m == 0 && k != 0)) {
+      const int i = atomicAdd(&sm.nlive, 1);
+      if (i < kLive) sm.live[i] = (unsigned short)j;
+    }
+  }
+  __syncthreads();
+  const int nlive = sm.nlive;
+  if (nlive == 0) return;
+  const bool listed = nlive <= kLive;
+  const int L = listed ? kThreads / ((nlive + kR - 1) / kR) : (int)it.L;
+  const int g = threadIdx.x / L, lane = threadIdx.x - g * L;
+  // context of slot r of this thread: the listed live contexts in list
+  // order, or the unit's contexts in index order (dead ones stay dead)
+  auto ctx_at = [&](int r) -> unsigned long long {
+    const int s = g * kR + r;
+    if (listed) return cbase + sm.live[s < nlive ? s : 0];
+    return cbase + (unsigned long long)(s < (int)ncu ? s : 0);
+  };
+  const int nslots = listed ? nlive : (int)ncu;
 
   W M[kR], K[kR], WX[kR][EE];
   unsigned valid = 0;
@@ -662,24 +722,17 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
   }
 #pragma unroll
   for (int r = 0; r < kR; ++r) {
-    const unsigned long long c = c0 + r < it.nctx ? c0 + r : c0;  // pad with a duplicate
-    if (c0 + r < it.nctx) valid |= 1u << r;
-    if (FUSED) {
-      const Ctx<W> cx = p.ctxs[it.ctx_off + (c < it.nctx ? c : 0)];
-      M[r] = cx.M;
-      K[r] = cx.K;
-      continue;
+    W wx[EE];
+    context_constraint<W, E, FUSED>(p, d, it, ctx_at(r), M[r], K[r], wx);
+    if (g * kR + r < nslots && !(M[r] == 0 && K[r] != 0)) {
+      valid |= 1u << r;
+    } else {  // padding and dead contexts: a constraint nothing satisfies
+      M[r] = 0;
+      K[r] = 1;
     }
-    W wl[kMaxDepth];
-    decode_context<W>(d, it, c, wl);
-    W m = (W)~W(0), k = d.target;
-    for (int l = 0; l < it.inv; ++l)
-      if (!invert_level<W>(it.lv[l], wl[l], m, k)) atomicOr(&p.flags[1], 1);
-    M[r] = m;
-    K[r] = k;
     if (E > 0) {
 #pragma unroll
-      for (int j = 0; j < EE; ++j) WX[r][j] = wl[it.inv + j];
+      for (int j = 0; j < EE; ++j) WX[r][j] = wx[j];
     }
   }
 
@@ -688,6 +741,7 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
   const unsigned long long v1 = umin64(v0 + it.vb, item_voff(it) + it.nv);
   const unsigned long long q0 = v0 / VW, q1 = (v1 + VW - 1) / VW;
   const uint4* V4 = reinterpret_cast<const uint4*>(V);
+  if (threadIdx.x == 0 && p.live) atomicAdd(p.live, (unsigned long long)nlive * (v1 - v0));
 
   // First pass on the low 32 bits only (64-bit words): the low half of every
   // level's result (bitwise operators, +, -, *, x -> +-x + c) depends only on
@@ -731,7 +785,7 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
       const unsigned m16 = (unsigned)M[r] & 0xFFFFu, k16 = (unsigned)K[r] & 0xFFFFu;
       Mp[r] = m16 | (m16 << 16);
       Kp[r] = k16 | (k16 << 16);
-      pass += __int_as_float((127 - __popc(m16)) << 23);  // 2^-bits
+      if (valid >> r & 1) pass += __int_as_float((127 - __popc(m16)) << 23);  // 2^-bits
     }
     use_pack = SIMBA_PACK_ALWAYS || __all_sync(0xFFFFFFFFu, 2.f * pass < 0.25f);
   }
@@ -783,13 +837,14 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
         W y = xs[e];
         if (E > 0) y = eval_explicit<W, E>(X, WX[r], y);
         const bool h = FULL ? (y == K[r]) : ((W)(y & M[r]) == K[r]);
-        if (h) pre_push<W>(p, d, sm, it, c0 + r, v, s_in, s_out);
+        if (h) pre_push<W>(p, d, sm, it, ctx_at(r), v, s_in, s_out);
       }
     }
   };
 
   // The bottom values are streamed with four 16-byte loads in flight (one
   // with explicit levels, for code size).
+  if (!valid) return;  // after the warp-wide vote: no live context in this thread
   unsigned long long q = q0 + lane;
   const unsigned long long step = (unsigned long long)L;
   if (E == 0) {
@@ -1963,6 +2018,7 @@ class Search final : public SearchSession {
     p.start_ns = sc + 3;
     p.flags = reinterpret_cast<int*>(sc + 4);
     p.hits = sc + 6;
+    p.live = sc + 8;
     p.preq = d_preq_.as<unsigned long long>();
     p.maxS = h_.S;
     p.maxK = h_.k;
@@ -1979,7 +2035,7 @@ class Search final : public SearchSession {
     // reset counter, best, evaluated, flags
     unsigned long long init[8] = {0, ~0ULL, 0, 0, 0, 0, 0, 0};
     SB_CUDA(cudaMemcpyAsync(d_scal_.p, init, 3 * sizeof(unsigned long long), cudaMemcpyHostToDevice, stream_));
-    SB_CUDA(cudaMemsetAsync(d_scal_.as<unsigned long long>() + 4, 0, 4 * sizeof(unsigned long long), stream_));
+    SB_CUDA(cudaMemsetAsync(d_scal_.as<unsigned long long>() + 4, 0, 5 * sizeof(unsigned long long), stream_));
     const bool spine_ok = o_.engine == 0 && s <= count_ok_max_;
     int T = std::min(Tcap_, s);
     bool use_naive = !spine_ok || (s > T && (s - 1) / 2 > T);
@@ -2124,7 +2180,7 @@ class Search final : public SearchSession {
       SB_CUDA(cudaGetLastError());
     }
     SB_CUDA(cudaEventRecord(ev1_, stream_));
-    SB_CUDA(cudaMemcpyAsync(h_scal_, d_scal_.p, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_));
+    SB_CUDA(cudaMemcpyAsync(h_scal_, d_scal_.p, 9 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_));
     SB_CUDA(cudaStreamSynchronize(stream_));
     float e = 0, ek = 0, ej = 0;
     SB_CUDA(cudaEventElapsedTime(&e, ev0_, ev1_));
@@ -2137,6 +2193,7 @@ class Search final : public SearchSession {
     const unsigned long long* hs = static_cast<unsigned long long*>(h_scal_);
     *best = hs[1];
     *evaluated += hs[2];
+    nested_live_ += hs[8];
     const double cand_total = use_naive ? (double)ct_.n[s][8] : [&] {
       double c = 0;
       for (auto& it : items) c += (double)it.nctx * (double)it.nv;
@@ -2173,6 +2230,7 @@ class Search final : public SearchSession {
     launches_ = 0;
     kernel_ms_ = 0.0;
     join_ms_ = nested_ms_ = join_cand_ = nested_cand_ = join_streamed_ = join_table_ = 0.0;
+    nested_live_ = 0;
     alg_ops_ = 0;
     stamp_start_kernel<<<1, 1, 0, stream_>>>(d_scal_.as<unsigned long long>() + 3);
     ++launches_;
@@ -2195,6 +2253,7 @@ class Search final : public SearchSession {
       out->nested_ms = nested_ms_;
       out->join_candidates = (uint64_t)join_cand_;
       out->nested_candidates = (uint64_t)nested_cand_;
+      out->nested_live_candidates = nested_live_;
       out->join_bytes_streamed = join_streamed_;
       out->join_table_bytes = join_table_;
       out->alg_ops = alg_ops_;
@@ -2256,13 +2315,14 @@ class Search final : public SearchSession {
   int launches_ = 0;
   double kernel_ms_ = 0.0;
   double join_ms_ = 0.0, nested_ms_ = 0.0, join_cand_ = 0.0, nested_cand_ = 0.0;
+  uint64_t nested_live_ = 0;  // candidates of live nested-compare contexts
   double join_streamed_ = 0.0, join_table_ = 0.0;
   uint64_t alg_ops_ = 0;
   int sms_ = 0, grid_ = 0, grid_naive_ = 0, grid_join_ = 0;
   size_t smem_bytes_ = 0, join_off_ = 0, smem_join_ = 0;
   DevBuf d_in_, d_out_, d_counts_, d_scal_, d_items_, d_small_, d_ctx_, d_insts_, d_preq_, d_jobs_;
   DevBuf d_tabs_[kMaxSize + 1];  // V_t of every sample, allocated when size t is first built
-  unsigned long long h_scal_[8] = {};
+  unsigned long long h_scal_[16] = {};
   int Tcap_ = 0, Tf_ = 0, built_ = 0, last_T_ = 0;
 };
 
