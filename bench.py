@@ -217,10 +217,13 @@ def roofline(kinds: dict, alg_ops: float, steps: int, int_peak: float, alu_peak:
     """Roofline of the search kernel per launch kind, per step.
 
     The spine kernel runs two launches per size.  Nested compares (spines
-    with & or |) decide each candidate with a masked 64-bit compare, 3
+    with & or |) decide the candidates of a context whose sample-0
+    constraint no bottom value satisfies by that constraint alone, and each
+    candidate of the other (live) contexts with a masked 64-bit compare, 3
     algorithmic 32-bit lane operations (two AND-XOR halves and their
-    combination), all on the ALU pipe: achieved = those lane operations /
-    the launch time, against the ALU pipe's measured peak (simba_alu_peak).
+    combination), all on the ALU pipe: achieved = the live candidates' lane
+    operations / the launch time, against the ALU pipe's measured peak
+    (simba_alu_peak).
     Hash-join launches (the other spines) read each bottom value once per
     block of contexts: achieved = the bottom tables' bytes, each counted once
     per size (the algorithmic minimum) / the launch time, against the
@@ -241,7 +244,8 @@ def roofline(kinds: dict, alg_ops: float, steps: int, int_peak: float, alu_peak:
               "candidates": kinds["nested_candidates"] / steps,
               "achieved": nested_ops / (nm / 1e3) / 1e12 if nm > 0 else None,
               "peak": alu_peak / 1e12, "peak_source": "measured live: simba_alu_peak (LOP3 chains)",
-              "alg_ops_per_candidate": nested_ops / max(1.0, kinds["nested_candidates"] / steps),
+              "live_candidates": kinds["nested_live_candidates"] / steps,
+              "alg_ops_per_live_candidate": nested_ops / max(1.0, kinds["nested_live_candidates"] / steps),
               "traffic": None}
     nested["frac"] = nested["achieved"] / nested["peak"] if nested["achieved"] else None
     nested["frac_of_int_peak"] = (nested["achieved"] * 1e12 / int_peak) if nested["achieved"] else None
@@ -427,6 +431,7 @@ def run_ours(a, rank: int, world: int, local_rank: int) -> None:
         e0.record(stream)
         kernel_ms, alg_ops, launches, evaluated = 0.0, 0, 0, 0
         kinds = {"join_ms": 0.0, "nested_ms": 0.0, "join_candidates": 0, "nested_candidates": 0,
+                 "nested_live_candidates": 0,
                  "join_bytes_streamed": 0.0, "join_table_bytes": 0.0}
         for _ in range(a.steps):
             r = sess.sweep(2, L)

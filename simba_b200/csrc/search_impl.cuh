@@ -132,10 +132,11 @@ struct alignas(16) Item {
   uint64_t vblocks;     // value blocks
   uint16_t cb;          // contexts per unit = G * kR (join: per block)
   int8_t joinable;      // every context's constraint is v & M == K with M a low-bit mask
-  int8_t pad0;
+  int8_t group;         // fused member: index of its group (live-context lists)
   uint16_t G, L;        // G context groups x L value lanes = kThreads
   int8_t depth, inv, bottom, full, nexp;
-  int8_t fused;         // 1: contexts are read from the materialised list
+  int8_t fused;         // 1: contexts are read from the materialised list; 2: the list
+                        // holds only the live contexts (see materialize_kernel)
   uint16_t cpu;         // context blocks per work unit (> 1 for small bottoms)
   uint64_t ctx_off;     // fused: first context in Params::ctxs
   uint32_t inst;        // instance (index into Params::insts)
@@ -240,6 +241,8 @@ struct Params {
   int* flags;  // [0] budget expired, [1] inversion failure, [2] queue overflows
   unsigned long long* hits;  // sample-0 matches sent to verification (may be null)
   unsigned long long* live;  // candidates of live nested-compare contexts (may be null)
+  unsigned long long* ctx_live;  // per fused group: [2g] live contexts appended, [2g+1] the
+                                 // group's first list slot (null: every context in place)
   unsigned long long* preq;  // per-CTA queues of sample-0 matches, [grid][kPreG] (may be null)
   unsigned join_off;         // byte offset of JoinSmem in dynamic shared memory; 0: no join units
   unsigned long long total_units;
@@ -288,6 +291,7 @@ struct alignas(16) JoinSmem {
   unsigned bits[kJoinBits / 32];
   unsigned char b[kJoinSlots];  // low-bit mask width of the slot's constraint
   unsigned long long mc;        // AND of the block's masks: the bits joined on
+  unsigned long long tag;       // item and context block the tables hold (~0: none)
 };
 
 static_assert(offsetof(Smem, item) % 16 == 0, "Smem::item must be 16-byte aligned");
@@ -681,20 +685,24 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
   // an & or | are such.  The live ones are listed in shared memory and, when
   // the list holds them all, the CTA's threads are laid out over them alone:
   // ceil(live / kR) groups, the rest of the threads as value lanes.
-  if (threadIdx.x == 0) sm.nlive = 0;
-  __syncthreads();
-  for (unsigned j = threadIdx.x; j < ncu; j += blockDim.x) {
-    W m, k;
-    context_constraint<W, E, FUSED>(p, d, it, cbase + j, m, k, nullptr);
-    if (!(m == 0 && k != 0)) {
-      const int i = atomicAdd(&sm.nlive, 1);
-      if (i < kLive) sm.live[i] = (unsigned short)j;
+  // A compacted context list (fused == 2) holds live contexts only.
+  const bool all_live = FUSED && it.fused == 2;
+  if (!all_live) {
+    if (threadIdx.x == 0) sm.nlive = 0;
+    __syncthreads();
+    for (unsigned j = threadIdx.x; j < ncu; j += blockDim.x) {
+      W m, k;
+      context_constraint<W, E, FUSED>(p, d, it, cbase + j, m, k, nullptr);
+      if (!(m == 0 && k != 0)) {
+        const int i = atomicAdd(&sm.nlive, 1);
+        if (i < kLive) sm.live[i] = (unsigned short)j;
+      }
     }
+    __syncthreads();
   }
-  __syncthreads();
-  const int nlive = sm.nlive;
+  const int nlive = all_live ? (int)ncu : sm.nlive;
   if (nlive == 0) return;
-  const bool listed = nlive <= kLive;
+  const bool listed = !all_live && nlive <= kLive;
   const int L = listed ? kThreads / ((nlive + kR - 1) / kR) : (int)it.L;
   const int g = threadIdx.x / L, lane = threadIdx.x - g * L;
   // context of slot r of this thread: the listed live contexts in list
@@ -929,7 +937,13 @@ __global__ void __launch_bounds__(256) materialize_kernel(Params<W> p, Ctx<W>* o
       if (!invert_level<W>(it.lv[l], wl[l], m, k)) atomicOr(&p.flags[1], 1);
     cx.M = m;
     cx.K = k;
-    out[gi] = cx;
+    if (p.ctx_live) {  // compacted lists: only contexts some bottom value can complete
+      if (m == 0 && k != 0) continue;
+      unsigned long long* gl = p.ctx_live + 2 * it.group;
+      out[gl[1] + atomicAdd(gl, 1ULL)] = cx;
+    } else {
+      out[gi] = cx;
+    }
   }
 }
 
@@ -995,10 +1009,17 @@ __device__ void process_unit_join(const Params<W>& p, const InstDesc<W>& d, Smem
   const unsigned long long vblk = local / it.cblocks, cblk = local - vblk * it.cblocks;
   const unsigned long long c0 = cblk * it.cb;
   const int nc = (int)umin64(it.cb, it.nctx - c0);
+  // The tables of a context block stay in shared memory for the CTA's next
+  // unit: a single search's units of one fused group with one context block
+  // (the largest bottom tables) then skip the whole build.
+  const unsigned long long tag =
+      p.tasks ? ~0ULL : ((unsigned long long)(unsigned)sm.next_item << 40 | cblk);
+  if (tag == ~0ULL || js.tag != tag) {
   for (int i = threadIdx.x; i < kJoinSlots; i += blockDim.x) js.ctx[i] = ~0u;
   for (int i = threadIdx.x; i < kJoinBits / 32; i += blockDim.x) js.bits[i] = 0u;
   if (threadIdx.x == 0) js.mc = ~0ULL;
   __syncthreads();
+  if (threadIdx.x == 0) js.tag = tag;  // every thread read the old tag before the barrier
   // 1. constraints of this thread's (at most two) contexts; the common mask
   W ms[2], ks[2];
   bool ok[2];
@@ -1024,18 +1045,14 @@ __device__ void process_unit_join(const Params<W>& p, const InstDesc<W>& d, Smem
     if (ok[r]) atomicAnd(&js.mc, (unsigned long long)m);
   }
   __syncthreads();
-  const unsigned long long mc = js.mc;
-  // the block joins on at least the low 32 bits (every mask keeps them: the
-  // usual case): the hash reads the low word alone, and the exact key
-  // compare on a filter hit settles the rest (same hash as join_hash for
-  // 32-bit words)
-  const bool lo32 = sizeof(W) == 4 || (unsigned)mc == 0xFFFFFFFFu;
+  const unsigned long long mc0 = js.mc;
+  const bool lo32b = sizeof(W) == 4 || (unsigned)mc0 == 0xFFFFFFFFu;
   // 2. filter bits and table entries, keyed on K & Mc
 #pragma unroll
   for (int r = 0; r < 2; ++r) {
     if (!ok[r]) continue;
     const int j = threadIdx.x + r * blockDim.x;
-    const unsigned hx = lo32 ? (unsigned)ks[r] * 0x85EBCA6Bu : join_hash((unsigned long long)ks[r] & mc);
+    const unsigned hx = lo32b ? (unsigned)ks[r] * 0x85EBCA6Bu : join_hash((unsigned long long)ks[r] & mc0);
     atomicOr(&js.bits[hx >> 23], 1u << ((hx >> 18) & 31));
     unsigned h = hx >> 22;
     for (int t = 0; t < kJoinSlots; ++t, h = (h + 1) & (kJoinSlots - 1)) {
@@ -1047,6 +1064,13 @@ __device__ void process_unit_join(const Params<W>& p, const InstDesc<W>& d, Smem
     }
   }
   __syncthreads();
+  }
+  const unsigned long long mc = js.mc;
+  // the block joins on at least the low 32 bits (every mask keeps them: the
+  // usual case): the hash reads the low word alone, and the exact key
+  // compare on a filter hit settles the rest (same hash as join_hash for
+  // 32-bit words)
+  const bool lo32 = sizeof(W) == 4 || (unsigned)mc == 0xFFFFFFFFu;
   // 3. probe with every bottom value of the block
   constexpr int VW = 16 / sizeof(W);
   const W* V = d.tab[it.bottom];
@@ -1172,6 +1196,7 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
     sm.inst_idx = -1;
     sm.lk_task = -1;
     sm.lk_item = -1;
+    if (js) js->tag = ~0ULL;
   }
   __syncthreads();
   for (;;) {
@@ -1727,17 +1752,22 @@ static inline float spine_prio(const Item& it, int size, const float* prior) {
 // each stream their bottom table once; spines sharing a bottom size (and
 // mask kind) are fused into one context list instead, materialised on the
 // device.  Returns the fused work items; `small` receives the member spines
-// with their offsets into the list.
+// with their offsets into the list.  With `nested_all`, every fully inverted
+// spine under an & or | is fused whatever its number of contexts (up to
+// max_ctxs in all), so that its list can be compacted to the live contexts.
 static inline void fuse_small(std::vector<Item>& items, std::vector<Item>* small, uint64_t* nctxs,
-                              const CountTable& ct, uint64_t max_ctxs, bool by_prio = false) {
+                              const CountTable& ct, uint64_t max_ctxs, bool by_prio = false,
+                              bool nested_all = false) {
   std::vector<Item> keep;
   std::vector<Item> groups;
   std::vector<std::vector<size_t>> members;
   uint64_t total = 0;
   for (auto& it : items) {
     // a class range of a tabled size covers part of its bottom table: not fused
-    const bool fusable = it.nexp == 0 && it.nctx < (uint64_t)kThreads * kR && total + it.nctx <= max_ctxs &&
-                         item_voff(it) == 0 && it.nv == ct.n[(int)it.bottom][8];
+    const bool fusable = it.nexp == 0 &&
+                         (it.nctx < (uint64_t)kThreads * kR || (nested_all && !it.joinable)) &&
+                         total + it.nctx <= max_ctxs && item_voff(it) == 0 &&
+                         it.nv == ct.n[(int)it.bottom][8];
     if (!fusable) {
       keep.push_back(it);
       continue;
@@ -1752,6 +1782,10 @@ static inline void fuse_small(std::vector<Item>& items, std::vector<Item>* small
           groups[gi].joinable == it.joinable &&
           (!by_prio || groups[gi].prio == it.prio))
         break;
+    if (gi == groups.size() && groups.size() >= 127) {  // group indices are int8_t
+      keep.push_back(it);
+      continue;
+    }
     if (gi == groups.size()) {
       Item g;
       memset(&g, 0, sizeof(g));
@@ -1760,12 +1794,14 @@ static inline void fuse_small(std::vector<Item>& items, std::vector<Item>* small
       g.joinable = it.joinable;
       g.prio = it.prio;
       g.fused = 1;
+      g.group = (int8_t)groups.size();
       g.nv = ct.n[(int)it.bottom][8];
       g.base = ~0ULL;
       groups.push_back(g);
       members.emplace_back();
     }
     members[gi].push_back(small->size());
+    it.group = (int8_t)gi;
     groups[gi].base = std::min(groups[gi].base, it.base);
     groups[gi].nctx += it.nctx;
     small->push_back(it);
@@ -2031,6 +2067,7 @@ class Search final : public SearchSession {
 
   int search_size(int s, bool stop, uint64_t* best, uint64_t* evaluated, double* ms, int shard = 0,
                   int nshards = 1) {
+    dead_ = 0;
     double alg_total = 0;
     // reset counter, best, evaluated, flags
     unsigned long long init[8] = {0, ~0ULL, 0, 0, 0, 0, 0, 0};
@@ -2079,8 +2116,66 @@ class Search final : public SearchSession {
           if (it.depth > 0) it.prio = spine_prio(it, s, o_.class_prior);
       std::vector<Item> small;
       uint64_t nctxs = 0;
-      fuse_small(items, &small, &nctxs, ct_, 1ULL << 22, guided);
-      const uint64_t unit_target = 1ULL << (o_.unit_log2 > 0 ? std::min(o_.unit_log2, 40) : 22);
+      fuse_small(items, &small, &nctxs, ct_, 1ULL << 22, guided, true);
+      for (auto& it : items) {  // planned work of the two launch kinds (every joinable spine joins)
+        const double c = (double)it.nctx * (double)it.nv;
+        if (it.joinable) join_cand_ += c;
+        else nested_cand_ += c;
+      }
+      Params<W> p = params(s);
+      SB_CUDA(cudaEventRecord(evk_, stream_));
+      double dead = 0;  // candidates of contexts left out of the compacted lists
+      if (nctxs) {
+        // Materialise the fused spines' contexts, keeping per group only the
+        // live ones (some bottom value may complete them on sample 0), and
+        // read the live counts back: the work units are laid out over those.
+        SB_CUDA(d_small_.reserve(small.size() * sizeof(Item)));
+        SB_CUDA(cudaMemcpyAsync(d_small_.p, small.data(), small.size() * sizeof(Item),
+                                cudaMemcpyHostToDevice, stream_));
+        SB_CUDA(d_ctx_.reserve(nctxs * sizeof(Ctx<W>)));
+        for (auto& it : items)
+          if (it.fused) {
+            h_glive_[2 * it.group] = 0;
+            h_glive_[2 * it.group + 1] = it.ctx_off;
+          }
+        SB_CUDA(d_glive_.reserve(sizeof(h_glive_)));
+        SB_CUDA(cudaMemcpyAsync(d_glive_.p, h_glive_, sizeof(h_glive_), cudaMemcpyHostToDevice, stream_));
+        p.sitems = d_small_.as<Item>();
+        p.nsitems = (int)small.size();
+        p.nctxs = nctxs;
+        p.ctx_live = d_glive_.as<unsigned long long>();
+        const int mb = (int)std::min<uint64_t>((nctxs + 255) / 256, (uint64_t)sms_ * 8);
+        materialize_kernel<W><<<mb, 256, 0, stream_>>>(p, d_ctx_.as<Ctx<W>>());
+        ++launches_;
+        SB_CUDA(cudaGetLastError());
+        SB_CUDA(cudaMemcpyAsync(h_glive_, d_glive_.p, sizeof(h_glive_), cudaMemcpyDeviceToHost, stream_));
+        SB_CUDA(cudaStreamSynchronize(stream_));
+        p.ctx_live = nullptr;
+        p.ctxs = d_ctx_.as<Ctx<W>>();
+        std::vector<Item> kept;
+        for (auto& it : items) {
+          if (it.fused) {
+            const uint64_t live = h_glive_[2 * it.group];
+            dead += (double)(it.nctx - live) * (double)it.nv;
+            it.nctx = live;
+            it.fused = 2;
+            if (live == 0) continue;
+          }
+          kept.push_back(it);
+        }
+        items.swap(kept);
+      }
+      uint64_t unit_target = 1ULL << (o_.unit_log2 > 0 ? std::min(o_.unit_log2, 40) : 22);
+      if (o_.unit_log2 <= 0) {
+        // By default the nested-compare units shrink (down to 2^16
+        // candidates) until the launch has four units per resident CTA: the
+        // compacted lists leave a size little work, and a few large units
+        // would run as long serial loops on a few SMs.
+        double nested = 0;
+        for (auto& it : items)
+          if (!it.joinable) nested += (double)it.nctx * (double)it.nv;
+        while (unit_target > (1ULL << 16) && nested < 4.0 * grid_ * (double)unit_target) unit_target >>= 1;
+      }
       for (auto& it : items) finish_layout(it, kThreads, unit_target, 1 << std::min(o_.lanes_log2, 8));
       if (guided)  // most likely shape classes first; ties in rank order
         std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) {
@@ -2107,20 +2202,16 @@ class Search final : public SearchSession {
         units_join = units;
         units = 0;
       }
-      SB_CUDA(d_items_.reserve(items.size() * sizeof(Item)));
-      SB_CUDA(cudaMemcpyAsync(d_items_.p, items.data(), items.size() * sizeof(Item),
-                              cudaMemcpyHostToDevice, stream_));
+      if (!items.empty()) {
+        SB_CUDA(d_items_.reserve(items.size() * sizeof(Item)));
+        SB_CUDA(cudaMemcpyAsync(d_items_.p, items.data(), items.size() * sizeof(Item),
+                                cudaMemcpyHostToDevice, stream_));
+      }
       for (auto& it : items) alg_total += item_alg_ops(it, sizeof(W));
-      {  // planned work of the two launch kinds
+      {  // what the join launch streams
         bool seen[kMaxSize + 1] = {};
-        for (size_t q = 0; q < items.size(); ++q) {
+        for (size_t q = 0; q < nj; ++q) {
           const Item& it = items[q];
-          const double c = (double)it.nctx * (double)it.nv;
-          if (q >= nj) {
-            nested_cand_ += c;
-            continue;
-          }
-          join_cand_ += c;
           join_streamed_ += (double)it.nv * sizeof(W) * (double)it.cblocks;
           if (!seen[(int)it.bottom]) {
             seen[(int)it.bottom] = true;
@@ -2128,27 +2219,13 @@ class Search final : public SearchSession {
           }
         }
       }
-      Params<W> p = params(s);
+      if (shard == 0) dead_ = dead;
       p.items = d_items_.as<Item>() + nj;
       p.nitems = (int)(items.size() - nj);
       p.total_units = units;
       p.unit_offset = (unsigned long long)shard;
       p.unit_stride = (unsigned long long)nshards;
       p.stop_on_match = stop ? (guided ? 2 : 1) : 0;
-      SB_CUDA(cudaEventRecord(evk_, stream_));
-      if (nctxs) {
-        SB_CUDA(d_small_.reserve(small.size() * sizeof(Item)));
-        SB_CUDA(cudaMemcpyAsync(d_small_.p, small.data(), small.size() * sizeof(Item),
-                                cudaMemcpyHostToDevice, stream_));
-        SB_CUDA(d_ctx_.reserve(nctxs * sizeof(Ctx<W>)));
-        p.sitems = d_small_.as<Item>();
-        p.nsitems = (int)small.size();
-        p.nctxs = nctxs;
-        const int mb = (int)std::min<uint64_t>((nctxs + 255) / 256, (uint64_t)sms_ * 8);
-        materialize_kernel<W><<<mb, 256, 0, stream_>>>(p, d_ctx_.as<Ctx<W>>());
-        ++launches_;
-        p.ctxs = d_ctx_.as<Ctx<W>>();
-      }
       if (nj) {
         Params<W> pj = p;
         pj.items = d_items_.as<Item>();
@@ -2192,7 +2269,9 @@ class Search final : public SearchSession {
     nested_ms_ += ek - ej;
     const unsigned long long* hs = static_cast<unsigned long long*>(h_scal_);
     *best = hs[1];
-    *evaluated += hs[2];
+    // the candidates the compaction decided count with a size swept to the
+    // end; where a match stopped the search early, only the units that ran
+    *evaluated += hs[2] + (hs[1] == ~0ULL ? (uint64_t)dead_ : 0);
     nested_live_ += hs[8];
     const double cand_total = use_naive ? (double)ct_.n[s][8] : [&] {
       double c = 0;
@@ -2321,6 +2400,9 @@ class Search final : public SearchSession {
   int sms_ = 0, grid_ = 0, grid_naive_ = 0, grid_join_ = 0;
   size_t smem_bytes_ = 0, join_off_ = 0, smem_join_ = 0;
   DevBuf d_in_, d_out_, d_counts_, d_scal_, d_items_, d_small_, d_ctx_, d_insts_, d_preq_, d_jobs_;
+  DevBuf d_glive_;                       // per fused group: live count, first slot
+  unsigned long long h_glive_[2 * 128] = {};
+  double dead_ = 0;  // candidates of this size decided by the list compaction
   DevBuf d_tabs_[kMaxSize + 1];  // V_t of every sample, allocated when size t is first built
   unsigned long long h_scal_[16] = {};
   int Tcap_ = 0, Tf_ = 0, built_ = 0, last_T_ = 0;

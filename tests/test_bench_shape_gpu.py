@@ -107,3 +107,20 @@ def test_golden_u64_reference_instances(oracle):
             continue
         p = infix_to_postfix(ref["expr"])
         assert (len(p), OPS.index(p[-1])) == (res.size, res.op)
+
+
+def test_unsat_sweep_accounting_at_bench_shape():
+    """The benchmarked sweep (sizes 2..12 here): every block is searched, the
+    candidates decided add up to the reference rule's count less the
+    unary-chain classes, and of the nested-compare candidates only those of
+    live contexts (a bottom value can complete their sample-0 constraint) are
+    compared one by one -- on a random target, a minority."""
+    from simba_b200.instances import make_instance
+    inst = make_instance(15, 3, 64, 1, word_bits=64, const_one=True, unsat=True)
+    res = S.solve(inst, 13)
+    assert res.status == S.NOT_FOUND
+    t = S.count_table(12, 4)
+    assert res.candidates == sum(int(t[s][8]) for s in range(2, 13))
+    assert 0.9 * res.candidates <= res.evaluated <= res.candidates
+    assert res.nested_candidates + res.join_candidates <= res.candidates
+    assert 0 < res.nested_live_candidates < res.nested_candidates / 2

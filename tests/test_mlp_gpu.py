@@ -105,7 +105,15 @@ def test_trained_proposal_beats_uniform_order():
         # the sizes below are swept completely and identically by both
         ratios.append(a.evaluated / b.evaluated)
     assert acc > 1.5 / 64  # better than chance
-    assert np.median(ratios) < 1.0, (np.median(ratios), acc, len(ratios))
+    # Where the match turns up in the first wave of work units both orders do
+    # the same work (ratio 1: most contexts under & and | are decided before
+    # any unit runs, which leaves many final sizes one wave of work).  Where
+    # the order changed the work, the trained prior must need fewer
+    # candidates more often than not, and fewer on (geometric) average.
+    r = np.asarray(ratios)
+    wins, losses = int(np.sum(r < 1.0)), int(np.sum(r > 1.0))
+    assert wins > losses, (wins, losses, acc, len(ratios))
+    assert float(np.exp(np.mean(np.log(r)))) < 1.0, (ratios, acc)
     p.close()
 
 
