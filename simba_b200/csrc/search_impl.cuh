@@ -850,13 +850,13 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
     }
   };
 
-  // The bottom values are streamed with four 16-byte loads in flight (one
-  // with explicit levels, for code size).
+  // The bottom values are streamed with four 16-byte loads in flight.
   if (!valid) return;  // after the warp-wide vote: no live context in this thread
   unsigned long long q = q0 + lane;
   const unsigned long long step = (unsigned long long)L;
-  if (E == 0) {
+  {
 #if SIMBA_NESTED_PIPELINE
+    if (E == 0) {
     // software pipeline: the next four loads are issued before the current
     // four are tested, so the tests overlap their latency
     if (q + 3 * step < q1) {
@@ -879,6 +879,7 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
       test(a2, q + 2 * step);
       test(a3, q + 3 * step);
       q += 4 * step;
+    }
     }
 #else
     for (; q + 3 * step < q1; q += 4 * step) {
@@ -1619,7 +1620,7 @@ static inline void finish_structure(Item& it, uint64_t mask) {
 // Thread layout and work units: G groups of kR contexts x L lanes over the
 // bottom values, about 2^22 candidates per unit.
 static inline void finish_layout(Item& it, int threads, uint64_t unit_target = 1ULL << 22,
-                                 int min_lanes = 1) {
+                                 int min_lanes = 1, uint64_t max_vals_per_lane = 0) {
   const uint64_t nctx = it.nctx;
   if (it.joinable && nctx >= kJoinMin) {  // hash join (full = 2)
     it.full = 2;
@@ -1646,6 +1647,9 @@ static inline void finish_layout(Item& it, int threads, uint64_t unit_target = 1
   uint64_t vb = unit_target / it.cb;  // about unit_target candidates per unit
   const uint64_t align = 64ULL * it.L;
   vb = std::max<uint64_t>(align, (vb + align - 1) / align * align);
+  // a cap on the bottom values one lane streams per unit keeps a unit's
+  // serial loop short where few contexts leave the thread layout mostly lanes
+  if (max_vals_per_lane && vb > max_vals_per_lane * it.L) vb = max_vals_per_lane * it.L;
   const uint64_t nv_al = (it.nv + 63) / 64 * 64;
   if (vb > nv_al) vb = nv_al;
   it.vb = vb;
@@ -2176,7 +2180,14 @@ class Search final : public SearchSession {
           if (!it.joinable) nested += (double)it.nctx * (double)it.nv;
         while (unit_target > (1ULL << 16) && nested < 4.0 * grid_ * (double)unit_target) unit_target >>= 1;
       }
-      for (auto& it : items) finish_layout(it, kThreads, unit_target, 1 << std::min(o_.lanes_log2, 8));
+      for (auto& it : items) {
+        // Nested spines left out of the compacted lists (explicit levels)
+        // find most of their contexts dead in each unit: units an eighth
+        // the size spread the live ones' streaming over more CTAs.
+        const bool listless = !it.joinable && !it.fused && it.depth > 0 && o_.unit_log2 <= 0;
+        const uint64_t ut = listless ? std::max<uint64_t>(unit_target >> 3, 1ULL << 16) : unit_target;
+        finish_layout(it, kThreads, ut, 1 << std::min(o_.lanes_log2, 8), o_.unit_log2 <= 0 ? 256 : 0);
+      }
       if (guided)  // most likely shape classes first; ties in rank order
         std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) {
           return a.prio != b.prio ? a.prio > b.prio : a.base < b.base;
