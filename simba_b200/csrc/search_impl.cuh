@@ -79,6 +79,9 @@ constexpr int kLive = 512;     // live contexts of a nested-compare unit listed 
 #ifndef SIMBA_PACK_IMAD
 #define SIMBA_PACK_IMAD 1  // packed prefilter: the subtraction as a multiply-add (FMA pipe)
 #endif
+#ifndef SIMBA_XOP_SPECIALIZE
+#define SIMBA_XOP_SPECIALIZE 1  // one explicit level: its operator as a template argument
+#endif                          // (a spine_kernel variant of its own; compile time grows)
 #ifndef SIMBA_JOIN_VALS_LOG2
 #define SIMBA_JOIN_VALS_LOG2 15  // hash join: bottom values per work unit
 #endif
@@ -668,7 +671,22 @@ __device__ __forceinline__ void context_constraint(const Params<W>& p, const Ins
   }
 }
 
-template <class W, int E, bool FULL, bool FUSED>
+// One explicit level with its operator fixed at compile time (XOP >= 0):
+// 0 &, 1 |, 2 ^, 3 +, 4 y - w, 5 w - y, 6 *, 7 y + c, 8 c - y.
+template <class W, int XOP>
+__device__ __forceinline__ W xop_apply(W c, W w, W y) {
+  if (XOP == 0) return y & w;
+  if (XOP == 1) return y | w;
+  if (XOP == 2) return y ^ w;
+  if (XOP == 3) return y + w;
+  if (XOP == 4) return y - w;
+  if (XOP == 5) return w - y;
+  if (XOP == 6) return y * w;
+  if (XOP == 7) return y + c;
+  return c - y;
+}
+
+template <class W, int E, bool FULL, bool FUSED, int XOP = -1>
 __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm, const Item& it,
                              unsigned long long local, const W* s_in, const W* s_out) {
   constexpr int VW = 16 / sizeof(W);
@@ -829,7 +847,7 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
             H wh[EE];
 #pragma unroll
             for (int j = 0; j < EE; ++j) wh[j] = (H)WX[r][j];
-            y = eval_explicit<H, E>(XH, wh, y);
+            y = XOP >= 0 ? xop_apply<H, (XOP < 0 ? 0 : XOP)>(XH.c[0], wh[0], y) : eval_explicit<H, E>(XH, wh, y);
           }
           h4[r & 3] |= FULL ? (y == (H)K[r]) : ((H)(y & (H)M[r]) == (H)K[r]);
         }
@@ -843,7 +861,8 @@ __device__ void process_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm,
       for (int r = 0; r < kR; ++r) {
         if (!(valid >> r & 1)) continue;
         W y = xs[e];
-        if (E > 0) y = eval_explicit<W, E>(X, WX[r], y);
+        if (E > 0)
+          y = XOP >= 0 ? xop_apply<W, (XOP < 0 ? 0 : XOP)>(X.c[0], WX[r][0], y) : eval_explicit<W, E>(X, WX[r], y);
         const bool h = FULL ? (y == K[r]) : ((W)(y & M[r]) == K[r]);
         if (h) pre_push<W>(p, d, sm, it, ctx_at(r), v, s_in, s_out);
       }
@@ -1116,7 +1135,7 @@ __device__ void process_unit_join(const Params<W>& p, const InstDesc<W>& d, Smem
   for (; q < q1; q += step) probe(__ldg(V4 + q), q);
 }
 
-template <class W>
+template <class W, int XS>
 __device__ void dispatch_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm, JoinSmem* js,
                               const Item& it, unsigned long long local, const W* s_in,
                               const W* s_out) {
@@ -1143,7 +1162,25 @@ __device__ void dispatch_unit(const Params<W>& p, const InstDesc<W>& d, Smem& sm
   }
   switch (e) {
     case 0: return process_unit<W, 0, false, false>(p, d, sm, it, local, s_in, s_out);
-    case 1: return process_unit<W, 1, false, false>(p, d, sm, it, local, s_in, s_out);
+    case 1: {  // the explicit level's operator as a template argument
+      if (!XS) return process_unit<W, 1, false, false>(p, d, sm, it, local, s_in, s_out);
+      const Level& Lx = it.lv[it.inv];
+      if (Lx.kind == 1) {
+        if (Lx.eps > 0) return process_unit<W, 1, false, false, 7>(p, d, sm, it, local, s_in, s_out);
+        return process_unit<W, 1, false, false, 8>(p, d, sm, it, local, s_in, s_out);
+      }
+      switch (Lx.op) {
+        case OP_AND: return process_unit<W, 1, false, false, 0>(p, d, sm, it, local, s_in, s_out);
+        case OP_OR: return process_unit<W, 1, false, false, 1>(p, d, sm, it, local, s_in, s_out);
+        case OP_XOR: return process_unit<W, 1, false, false, 2>(p, d, sm, it, local, s_in, s_out);
+        case OP_ADD: return process_unit<W, 1, false, false, 3>(p, d, sm, it, local, s_in, s_out);
+        case OP_SUB:
+          if (Lx.small_left) return process_unit<W, 1, false, false, 5>(p, d, sm, it, local, s_in, s_out);
+          return process_unit<W, 1, false, false, 4>(p, d, sm, it, local, s_in, s_out);
+        case OP_MUL: return process_unit<W, 1, false, false, 6>(p, d, sm, it, local, s_in, s_out);
+        default: return process_unit<W, 1, false, false>(p, d, sm, it, local, s_in, s_out);
+      }
+    }
     default: return process_unit<W, 2, false, false>(p, d, sm, it, local, s_in, s_out);
   }
 }
@@ -1180,7 +1217,7 @@ __device__ W* load_instance(const Params<W>& p, Smem& sm, int idx, W* s_in) {
 }
 
 // Persistent search kernel: CTAs take work units from an atomic counter.
-template <class W>
+template <class W, int XS = SIMBA_XOP_SPECIALIZE>
 __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
@@ -1304,7 +1341,7 @@ __global__ void SIMBA_SPINE_BOUNDS spine_kernel(Params<W> p) {
       const unsigned long long b0 = cu * cpu, b1 = umin64(b0 + cpu, it.cblocks);
       for (unsigned long long b = b0; b < b1; ++b) {
         const unsigned long long lb = it.full == 2 ? vblk * it.cblocks + b : b * it.vblocks + vblk;
-        dispatch_unit<W>(p, d, sm, js, it, lb, s_in, s_out);
+        dispatch_unit<W, XS>(p, d, sm, js, it, lb, s_in, s_out);
         if (threadIdx.x == 0) {
           const unsigned long long c0 = b * it.cb, c1 = umin64(c0 + it.cb, it.nctx);
           const unsigned long long v0 = vblk * it.vb, v1 = umin64(v0 + it.vb, it.nv);  // a count

@@ -34,6 +34,9 @@
 #include <mutex>
 #include <vector>
 
+// the static entry point runs sizes with small tables: the generic explicit
+// level keeps this unit's compile time down (and its kernel a symbol of its own)
+#define SIMBA_XOP_SPECIALIZE 0
 #include "search_impl.cuh"
 
 namespace simba {
